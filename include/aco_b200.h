@@ -1,0 +1,149 @@
+#ifndef ACO_B200_H
+#define ACO_B200_H
+
+#include "aco_api.h"
+
+/*
+ * aco_b200.h -- the thin C ABI of the B200 ACO-for-CVRP hot path.
+ *
+ * Plain C types only.  Host buffers are owned by the caller; device buffers
+ * are owned by the context.  One context drives one instance on one GPU
+ * through one CUDA stream; a context is used by one host thread at a time.
+ * Every function returns an int status: 0 (ACO_OK) or an AcoStatus code
+ * (include/aco.h).
+ *
+ * What each entry point replaces in the reference:
+ *   aco_b200_setup        the set-up half of aco_vrp_cuda_with_capacity
+ *                         (src/cuda/aco_cuda.cu:198-292: parameters, device
+ *                         buffers, launch_init_tau, launch_build_candidate_lists)
+ *   aco_b200_run          the epoch loop (aco_cuda.cu:331-429), run on the
+ *                         device in CUDA-graph chunks with device-side stop
+ *                         rules instead of 7 host synchronisations per epoch
+ *   aco_b200_get_best     copy_ant_to_solution + the final D2H
+ *                         (aco_cuda.cu:138-168, :367-380)
+ *   aco_b200_construct    one launch of kernel_construct_solutions
+ *                         (include/aco_cuda_kernels.h:104-115) on the current
+ *                         pheromone, for parity checks
+ *   aco_b200_evaporate_deposit  kernel_evaporate_tau + kernel_deposit_solution
+ *                         + kernel_deposit_flat_solution (aco_cuda.cu:385-396)
+ *   aco_b200_get_tau / set_tau / get_candidates / get_weights / get_ants /
+ *   get_state             read-outs of the device state for the tests (the
+ *                         reference has none; its tests are end-to-end only)
+ */
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct aco_b200_ctx aco_b200_ctx;
+
+/* Problem and run parameters (the reference's solver arguments plus the
+ * ACO_SOLVER_* configuration, src/common/aco_config.c:33-73). */
+typedef struct {
+  int n;                      /* customers; nodes are 0 (depot) .. n      */
+  int K;                      /* vehicles                                  */
+  long long capacity;         /* per vehicle, in demand units              */
+  int ants;                   /* m; 0 selects 256 (aco_cuda.cu:206)        */
+  int cand_k;                 /* 0 selects 32, or n when n <= 32 (:198-199) */
+  const float *x;             /* [n+1] host                                */
+  const float *y;             /* [n+1] host                                */
+  const int *demand;          /* [n+1] host, NULL = unit demand            */
+  double alpha, beta, rho, tau0, Q;
+  unsigned int seed;
+  int stagnation_epochs;      /* 0 = no stagnation stop                    */
+  int fixed_epochs;           /* 0 = no epoch limit                        */
+  double min_rel_improvement; /* fraction (the env variable is percent)    */
+  double timeout_seconds;     /* 0 = none                                  */
+} aco_b200_problem;
+
+/* Device-side solver state after a run. */
+typedef struct {
+  int epochs;                 /* epochs completed                          */
+  int iter_since_best;        /* epochs since the last significant gain    */
+  int stopped;                /* nonzero: a stop rule fired                */
+  int stop_reason;            /* bit 1 stagnation, 2 fixed, 4 timeout      */
+  int found;                  /* last epoch had a feasible ant             */
+  int improved;               /* last epoch improved the global best       */
+  int best_ant;               /* last epoch's iteration-best ant           */
+  int error;                  /* device error flag (0 = none)              */
+  double global_best;         /* DBL_MAX while no feasible solution        */
+  double iter_best;           /* last epoch's iteration-best cost          */
+  float dep_iter, dep_global; /* last epoch's deposit amounts              */
+  unsigned long long total_steps; /* ant-steps (moves) since set-up        */
+} aco_b200_state;
+
+/* One record per epoch, for the progress lines (aco_cuda.cu:39-74). */
+typedef struct {
+  int epoch;                  /* 1-based, as printed by the reference      */
+  int iter_since_best;
+  int improved;
+  int found;
+  double global_best;
+  unsigned long long elapsed_ns;
+} aco_b200_epoch_record;
+
+ACO_API int aco_b200_create(aco_b200_ctx **out, int device);
+ACO_API int aco_b200_destroy(aco_b200_ctx *ctx);
+/* Use an external stream (e.g. a framework's current stream); NULL = own. */
+ACO_API int aco_b200_set_stream(aco_b200_ctx *ctx, void *cuda_stream);
+
+/* Uploads the instance, builds candidate lists and eta levels on the device,
+ * initialises the pheromone matrix and the run state. */
+ACO_API int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *problem);
+
+/* Runs up to max_epochs more epochs (stops earlier on a stop rule); fills
+ * *state.  Epoch records since the last call are returned through
+ * records/n_records when records is not NULL (capacity max_records). */
+ACO_API int aco_b200_run(aco_b200_ctx *ctx, int max_epochs, aco_b200_state *state,
+                 aco_b200_epoch_record *records, int max_records,
+                 int *n_records);
+
+/* Enqueues max_epochs epochs on the context stream without synchronising
+ * (for timing with events on that stream). */
+ACO_API int aco_b200_enqueue_epochs(aco_b200_ctx *ctx, int epochs);
+ACO_API int aco_b200_synchronize(aco_b200_ctx *ctx);
+
+/* Runs `epochs` epochs with one CUDA event between consecutive kernels on
+ * the context stream and adds each kernel's device time (ms) into
+ * kernel_ms[4]: weights, construct, best, evaporate+deposit. */
+ACO_API int aco_b200_profile_epochs(aco_b200_ctx *ctx, int epochs, float *kernel_ms);
+
+/* Best solution so far in compact form: K segments [0 c.. 0] back to back
+ * (nodes capacity n + 2K), the K segment lengths and the FP64 cost. */
+ACO_API int aco_b200_get_best(aco_b200_ctx *ctx, int *nodes, int *lens, double *cost);
+
+ACO_API int aco_b200_get_state(aco_b200_ctx *ctx, aco_b200_state *state);
+ACO_API int aco_b200_get_dims(aco_b200_ctx *ctx, int *n, int *K, int *k, int *m);
+
+/* Test hooks (parity checks against the oracle). */
+ACO_API int aco_b200_get_tau(aco_b200_ctx *ctx, uint8_t *tau);       /* (n+1)^2 */
+ACO_API int aco_b200_set_tau(aco_b200_ctx *ctx, const uint8_t *tau); /* (n+1)^2 */
+ACO_API int aco_b200_get_candidates(aco_b200_ctx *ctx, int *cand, uint16_t *levels);
+ACO_API int aco_b200_get_tables(aco_b200_ctx *ctx, int32_t *A, uint32_t *lut,
+                        float *thresholds, int n_thresholds);
+/* Weights recomputed from the current pheromone ((n+1) k values). */
+ACO_API int aco_b200_get_weights(aco_b200_ctx *ctx, uint32_t *w);
+/* One construct pass for epoch number `epoch` on the current pheromone;
+ * per-ant results through aco_b200_get_ants.  layout: -1 = automatic,
+ * 0 = shared-memory weights, 1 = shared-memory packed levels, 2 = global. */
+ACO_API int aco_b200_construct(aco_b200_ctx *ctx, int epoch, int layout);
+ACO_API int aco_b200_get_ants(aco_b200_ctx *ctx, int *nodes /* m (n+2K) */,
+                      int *lens /* m K */, double *cost, int *feasible,
+                      int *steps, uint32_t *draws);
+/* Evaporation then deposit of the given iteration-best ant and of the
+ * given global-best solution (compact form), with the given amounts. */
+ACO_API int aco_b200_evaporate_deposit(aco_b200_ctx *ctx, int best_ant,
+                               float dep_iter, const int *gbest_nodes,
+                               const int *gbest_lens, float dep_global);
+
+/* Library build information. */
+ACO_API const char *aco_b200_build_info(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,296 @@
+"""ctypes binding of the C ABI in ``include/aco_b200.h``.
+
+The shared library ``libaco_b200.so`` is built in-tree (``make lib`` or
+``__graft_entry__.build()``).  There is no fallback: if the library is missing
+or no CUDA device is present, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Tuple
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libaco_b200.so")
+
+ACO_OK = 0
+ACO_ERR_INVALID_INPUT = 1
+ACO_ERR_ALLOCATION = 2
+ACO_ERR_NO_SOLUTION = 3
+ACO_ERR_BACKEND = 4
+
+LAYOUT_AUTO, LAYOUT_SMEM_WEIGHTS, LAYOUT_SMEM_PACKED, LAYOUT_GLOBAL = -1, 0, 1, 2
+N_THRESHOLDS = 4095
+
+# Every symbol include/aco_b200.h and include/aco.h declare.
+EXPORTED = [
+    "aco_b200_create", "aco_b200_destroy", "aco_b200_set_stream", "aco_b200_setup",
+    "aco_b200_run", "aco_b200_enqueue_epochs", "aco_b200_synchronize",
+    "aco_b200_get_best", "aco_b200_get_state", "aco_b200_get_dims",
+    "aco_b200_get_tau", "aco_b200_set_tau", "aco_b200_get_candidates",
+    "aco_b200_get_tables", "aco_b200_get_weights", "aco_b200_construct",
+    "aco_b200_get_ants", "aco_b200_evaporate_deposit", "aco_b200_build_info",
+    "aco_b200_profile_epochs",
+    "aco_status_string", "aco_vrp_cuda_with_capacity", "aco_vrp_cuda_with_demands",
+    "solution_create", "solution_free", "solution_reset", "solution_copy",
+    "solution_cost", "route_append", "solution_validate",
+    "vrp_load_tsplib_euc2d_coords", "vrp_load_tsplib_euc2d_coords_demands",
+    "aco_runtime_config_defaults", "aco_runtime_config_load_env",
+    "aco_parse_min_rel_improvement_percent", "cli_parse_int_arg",
+    "cli_parse_uint_arg", "cli_print_solution_routes", "cli_print_solution_cost",
+    "cli_validate_solution_or_report",
+]
+
+
+class AcoError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        names = {1: "invalid input", 2: "allocation failure", 3: "no solution",
+                 4: "backend failure"}
+        super().__init__(f"{where}: {names.get(status, 'status %d' % status)}")
+        self.status = status
+
+
+class Problem(C.Structure):
+    _fields_ = [("n", C.c_int), ("K", C.c_int), ("capacity", C.c_longlong),
+                ("ants", C.c_int), ("cand_k", C.c_int),
+                ("x", C.c_void_p), ("y", C.c_void_p), ("demand", C.c_void_p),
+                ("alpha", C.c_double), ("beta", C.c_double), ("rho", C.c_double),
+                ("tau0", C.c_double), ("Q", C.c_double), ("seed", C.c_uint),
+                ("stagnation_epochs", C.c_int), ("fixed_epochs", C.c_int),
+                ("min_rel_improvement", C.c_double), ("timeout_seconds", C.c_double)]
+
+
+class State(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("iter_since_best", C.c_int),
+                ("stopped", C.c_int), ("stop_reason", C.c_int), ("found", C.c_int),
+                ("improved", C.c_int), ("best_ant", C.c_int), ("error", C.c_int),
+                ("global_best", C.c_double), ("iter_best", C.c_double),
+                ("dep_iter", C.c_float), ("dep_global", C.c_float),
+                ("total_steps", C.c_ulonglong)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class EpochRecord(C.Structure):
+    _fields_ = [("epoch", C.c_int), ("iter_since_best", C.c_int),
+                ("improved", C.c_int), ("found", C.c_int),
+                ("global_best", C.c_double), ("elapsed_ns", C.c_ulonglong)]
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load():
+    """Loads libaco_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `make lib` (or "
+            "__graft_entry__.build()); there is no CPU fallback")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, f32 = C.c_void_p, C.c_int, C.c_float
+    sigs = {
+        "aco_b200_create": [vp, i32], "aco_b200_destroy": [vp],
+        "aco_b200_set_stream": [vp, vp], "aco_b200_setup": [vp, vp],
+        "aco_b200_run": [vp, i32, vp, vp, i32, vp],
+        "aco_b200_enqueue_epochs": [vp, i32], "aco_b200_synchronize": [vp],
+        "aco_b200_get_best": [vp, vp, vp, vp], "aco_b200_get_state": [vp, vp],
+        "aco_b200_get_dims": [vp, vp, vp, vp, vp],
+        "aco_b200_get_tau": [vp, vp], "aco_b200_set_tau": [vp, vp],
+        "aco_b200_get_candidates": [vp, vp, vp],
+        "aco_b200_get_tables": [vp, vp, vp, vp, i32],
+        "aco_b200_get_weights": [vp, vp], "aco_b200_construct": [vp, i32, i32],
+        "aco_b200_get_ants": [vp, vp, vp, vp, vp, vp, vp],
+        "aco_b200_evaporate_deposit": [vp, i32, f32, vp, vp, f32],
+        "aco_b200_profile_epochs": [vp, i32, vp],
+    }
+    for name, args in sigs.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = i32
+    L.aco_b200_build_info.restype = C.c_char_p
+    L.aco_status_string.restype = C.c_char_p
+    L.aco_status_string.argtypes = [i32]
+    _lib = L
+    return L
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != ACO_OK:
+        raise AcoError(rc, where)
+
+
+class Context:
+    """One instance on one GPU (aco_b200_ctx)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load()
+        self._h = C.c_void_p()
+        _check(self._lib.aco_b200_create(C.byref(self._h), device), "aco_b200_create")
+        self._keep = []
+        self.n = self.K = self.k = self.m = 0
+
+    def close(self):
+        if self._h:
+            self._lib.aco_b200_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_handle: int) -> None:
+        _check(self._lib.aco_b200_set_stream(self._h, C.c_void_p(stream_handle)),
+               "aco_b200_set_stream")
+
+    def setup(self, x, y, K: int, capacity: int, demand=None, ants: int = 256,
+              cand_k: int = 0, alpha=1.0, beta=2.0, rho=0.5, tau0=1.0, Q=1.0,
+              seed: int = 1234, stagnation_epochs: int = 0, fixed_epochs: int = 0,
+              min_rel_improvement: float = 1e-3, timeout_seconds: float = 0.0):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        d = None if demand is None else np.ascontiguousarray(demand, np.int32)
+        self._keep = [x, y, d]
+        p = Problem(n=len(x) - 1, K=K, capacity=int(capacity), ants=ants, cand_k=cand_k,
+                    x=_p(x).value, y=_p(y).value, demand=None if d is None else _p(d).value,
+                    alpha=alpha, beta=beta, rho=rho, tau0=tau0, Q=Q, seed=seed & 0xffffffff,
+                    stagnation_epochs=stagnation_epochs, fixed_epochs=fixed_epochs,
+                    min_rel_improvement=min_rel_improvement, timeout_seconds=timeout_seconds)
+        _check(self._lib.aco_b200_setup(self._h, C.byref(p)), "aco_b200_setup")
+        n, K_, k, m = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(self._lib.aco_b200_get_dims(self._h, C.byref(n), C.byref(K_), C.byref(k),
+                                            C.byref(m)), "aco_b200_get_dims")
+        self.n, self.K, self.k, self.m = n.value, K_.value, k.value, m.value
+        return self
+
+    def setup_instance(self, inst, **kw):
+        demand = None if inst.is_unit_demand() else inst.demand
+        return self.setup(inst.x, inst.y, inst.vehicles, inst.capacity, demand=demand, **kw)
+
+    def run(self, max_epochs: int, want_records: bool = False):
+        st = State()
+        recs = (EpochRecord * max(1, max_epochs))() if want_records else None
+        nrec = C.c_int(0)
+        _check(self._lib.aco_b200_run(self._h, max_epochs, C.byref(st),
+                                      recs, max_epochs if want_records else 0,
+                                      C.byref(nrec)), "aco_b200_run")
+        if want_records:
+            return st, [recs[i] for i in range(nrec.value)]
+        return st
+
+    def enqueue_epochs(self, epochs: int) -> None:
+        _check(self._lib.aco_b200_enqueue_epochs(self._h, epochs), "aco_b200_enqueue_epochs")
+
+    def profile_epochs(self, epochs: int) -> np.ndarray:
+        """Per-kernel device ms summed over `epochs` epochs:
+        [weights, construct, best, evaporate+deposit]."""
+        ms = np.zeros(4, np.float32)
+        _check(self._lib.aco_b200_profile_epochs(self._h, epochs, _p(ms)),
+               "aco_b200_profile_epochs")
+        return ms
+
+    def synchronize(self) -> None:
+        _check(self._lib.aco_b200_synchronize(self._h), "aco_b200_synchronize")
+
+    def state(self) -> State:
+        st = State()
+        _check(self._lib.aco_b200_get_state(self._h, C.byref(st)), "aco_b200_get_state")
+        return st
+
+    def best(self) -> Tuple[np.ndarray, np.ndarray, float]:
+        nodes = np.zeros(self.n + 2 * self.K, np.int32)
+        lens = np.zeros(self.K, np.int32)
+        cost = C.c_double()
+        rc = self._lib.aco_b200_get_best(self._h, _p(nodes), _p(lens), C.byref(cost))
+        if rc == ACO_ERR_NO_SOLUTION:
+            return nodes[:0], lens, float("inf")
+        _check(rc, "aco_b200_get_best")
+        return nodes[: int(lens.sum())].copy(), lens, cost.value
+
+    def tau(self) -> np.ndarray:
+        t = np.zeros((self.n + 1) * (self.n + 1), np.uint8)
+        _check(self._lib.aco_b200_get_tau(self._h, _p(t)), "aco_b200_get_tau")
+        return t
+
+    def set_tau(self, tau: np.ndarray) -> None:
+        t = np.ascontiguousarray(tau, np.uint8)
+        assert t.size == (self.n + 1) ** 2
+        _check(self._lib.aco_b200_set_tau(self._h, _p(t)), "aco_b200_set_tau")
+
+    def candidates(self) -> Tuple[np.ndarray, np.ndarray]:
+        cnt = (self.n + 1) * self.k
+        cand = np.zeros(cnt, np.int32)
+        lvl = np.zeros(cnt, np.uint16)
+        _check(self._lib.aco_b200_get_candidates(self._h, _p(cand), _p(lvl)),
+               "aco_b200_get_candidates")
+        return cand, lvl
+
+    def tables(self):
+        A = np.zeros(256, np.int32)
+        lut = np.zeros(256, np.uint32)
+        thr = np.zeros(N_THRESHOLDS, np.float32)
+        _check(self._lib.aco_b200_get_tables(self._h, _p(A), _p(lut), _p(thr), N_THRESHOLDS),
+               "aco_b200_get_tables")
+        return A, lut, thr
+
+    def weights(self) -> np.ndarray:
+        w = np.zeros((self.n + 1) * self.k, np.uint32)
+        _check(self._lib.aco_b200_get_weights(self._h, _p(w)), "aco_b200_get_weights")
+        return w
+
+    def construct(self, epoch: int, layout: int = LAYOUT_AUTO) -> None:
+        _check(self._lib.aco_b200_construct(self._h, epoch, layout), "aco_b200_construct")
+
+    def ants(self):
+        R = self.n + 2 * self.K
+        nodes = np.zeros(self.m * R, np.int32)
+        lens = np.zeros(self.m * self.K, np.int32)
+        cost = np.zeros(self.m, np.float64)
+        feas = np.zeros(self.m, np.int32)
+        steps = np.zeros(self.m, np.int32)
+        draws = np.zeros(self.m, np.uint32)
+        _check(self._lib.aco_b200_get_ants(self._h, _p(nodes), _p(lens), _p(cost), _p(feas),
+                                           _p(steps), _p(draws)), "aco_b200_get_ants")
+        return (nodes.reshape(self.m, R), lens.reshape(self.m, self.K), cost, feas, steps,
+                draws)
+
+    def evaporate_deposit(self, best_ant: int, dep_iter: float, gbest_nodes=None,
+                          gbest_lens=None, dep_global: float = 0.0) -> None:
+        gn = None if gbest_nodes is None else np.ascontiguousarray(gbest_nodes, np.int32)
+        gl = None if gbest_lens is None else np.ascontiguousarray(gbest_lens, np.int32)
+        _check(self._lib.aco_b200_evaporate_deposit(self._h, best_ant, dep_iter, _p(gn),
+                                                    _p(gl), dep_global),
+               "aco_b200_evaporate_deposit")
+
+
+def build_info() -> str:
+    return load().aco_b200_build_info().decode()
+
+
+def split_routes(nodes: np.ndarray, lens: np.ndarray) -> List[List[int]]:
+    out, off = [], 0
+    for ln in lens:
+        out.append([int(v) for v in nodes[off:off + int(ln)]])
+        off += int(ln)
+    return out

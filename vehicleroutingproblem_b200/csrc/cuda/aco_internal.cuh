@@ -1,0 +1,284 @@
+// aco_internal.cuh -- structures shared by the host solver and the kernels,
+// and the device helpers of the B200 ACO-for-CVRP hot path.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace acob200 {
+
+// ---------------------------------------------------------------------------
+// Integer selection weights.  A candidate t of row i gets the level
+//   e = A[q] - L,  A[q] = round(alpha q step G / ln 2),  L = #{T_j <= d^2}
+// with G = 16 levels per octave, and the weight
+//   w = LUT[min(emax_i - e, 255)],  LUT[r] = round(2^23 2^(-r/G)), LUT[255] = 0
+// where emax_i is the largest level of the row.  w < 2^24, a row of at most
+// 32 weights sums below 2^29, and a 24-bit draw r times that sum is below
+// 2^53: the roulette below is exact in integers and in the FP64 arithmetic
+// of the reference's select_next_customer (src/seq/aco_sequential.c:505-561).
+// ---------------------------------------------------------------------------
+constexpr int kLevelsPerOctave = 16;
+constexpr int kRelMax = 255;
+constexpr int kThresholds = 4095;
+constexpr int kMaxCand = 32;
+constexpr int kDrawBits = 24;
+constexpr uint32_t kDrawKey1 = 0x5EEDC0DEu;
+constexpr unsigned kFull = 0xffffffffu;
+
+// Stop-rule bits (DevState::stop_flags).
+constexpr int kStopStagnation = 1;
+constexpr int kStopFixed = 2;
+constexpr int kStopTimeout = 4;
+constexpr int kStopRunLimit = 8;
+
+// Device error bits (DevState::error).
+constexpr int kErrStageTimeout = 1;
+
+// Construct table layouts.
+constexpr int kLayoutSmemWeights = 0;  // cand u16 + w u32 staged in smem
+constexpr int kLayoutSmemPacked = 1;   // cand u16 + rel u8 + LUT in smem
+constexpr int kLayoutGlobal = 2;       // rows read from global memory (L2)
+
+struct EpochRec {
+  int epoch;
+  int iter_since_best;
+  int improved;
+  int found;
+  double global_best;
+  unsigned long long elapsed_ns;
+};
+
+constexpr int kLogCap = 1024;
+
+// Run state of one solve, resident on the device.  The epoch loop of the
+// reference (src/cuda/aco_cuda.cu:331-429) keeps these on the host; here the
+// kernels update them so that whole epochs run without host round trips.
+struct DevState {
+  int stop_flags;          // kStop* bits; nonzero: the next epoch is skipped
+  int skip;                // this epoch is skipped (set by the weights kernel)
+  int epoch;               // epochs completed
+  int iter_since_best;
+  int found;               // this epoch had a feasible ant
+  int improved;            // this epoch improved the global best
+  int best_ant;
+  int error;
+  double global_best;
+  double iter_best;
+  float dep_iter;
+  float dep_global;
+  unsigned long long total_steps;
+  unsigned long long start_ns;
+  // configuration
+  int stagnation;
+  int fixed_epochs;
+  int run_limit;
+  int log_count;
+  double min_rel;
+  unsigned long long timeout_ns;
+  float Qs;                // Q * 100 (src/cuda/aco_cuda.cu:228)
+  int pad0;
+};
+
+// Byte offsets of the construct kernel's dynamic shared memory.
+struct SmemPlan {
+  uint32_t off_cand, off_w, off_coords, off_dem, off_lut, off_vis;
+  uint32_t bytes_cand, bytes_w, bytes_coords, bytes_dem;
+  uint32_t total;
+  int vis_words;           // 32-bit words per ant bitmap
+  int wpb;                 // warps (ants) per block
+  int layout;
+};
+
+struct InstanceView {
+  int n, K, k, m;
+  long long cap;
+  long long total_demand;
+  int unit;                // 1: every customer has demand 1
+  int route_stride;        // n + 2K
+  const float2 *coords;    // [n+1]
+  const int *demand;       // [n+1]
+  const uint16_t *cand;    // [(n+1) k]
+  const uint16_t *lvl;     // [(n+1) k]
+};
+
+struct AntBuffers {
+  int *routes;             // [m][n + 2K] compact routes
+  int *lens;               // [m][K]
+  double *cost;            // [m]
+  int *feasible;           // [m]
+  int *steps;              // [m]
+  uint32_t *draws;         // [m]
+  long long *loads;        // [m][K]  per-vehicle load (repair scratch)
+  int *rep;                // [m][n]  repair additions (scratch)
+  int *repc;               // [m][K]  repair additions per vehicle (scratch)
+};
+
+struct EpochTables {
+  uint32_t *w;             // [(n+1) k] weights
+  uint8_t *rel;            // [(n+1) k] weight levels below the row maximum
+  const int32_t *A;        // [256]
+  const uint32_t *lut;     // [256]
+};
+
+struct PheromoneView {
+  uint8_t *tau;            // [(n+1)^2], row stride n+1
+  unsigned long long total;
+  float log_min, log_step;
+  uint8_t q_min, q_max, delta, pad;
+};
+
+// ---------------------------------------------------------------------------
+// Launch wrappers (aco_kernels.cu).
+// ---------------------------------------------------------------------------
+cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
+                              const float *thr, int J, uint16_t *cand,
+                              uint16_t *lvl, cudaStream_t s);
+cudaError_t launch_fill_u8(uint8_t *p, unsigned long long count, uint8_t v,
+                           cudaStream_t s);
+cudaError_t launch_weights(const InstanceView &iv, const PheromoneView &pv,
+                           const EpochTables &et, DevState *st, cudaStream_t s);
+cudaError_t launch_construct(const InstanceView &iv, const EpochTables &et,
+                             const AntBuffers &ab, const SmemPlan &plan,
+                             DevState *st, uint32_t seed, uint32_t epoch,
+                             uint32_t stream_id, int use_state_epoch,
+                             cudaStream_t s);
+cudaError_t launch_best(const InstanceView &iv, const AntBuffers &ab,
+                        DevState *st, int *gbest_nodes, int *gbest_lens,
+                        EpochRec *log, cudaStream_t s);
+cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
+                                const AntBuffers &ab, DevState *st,
+                                const int *gbest_nodes, const int *gbest_lens,
+                                unsigned int *counter, int grid,
+                                cudaStream_t s);
+cudaError_t launch_set_run_limit(DevState *st, int limit, cudaStream_t s);
+int construct_max_smem();
+cudaError_t prepare_construct_kernels();
+SmemPlan plan_construct(const InstanceView &iv, int layout, int num_sms,
+                        int max_smem);
+
+}  // namespace acob200
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+#ifdef __CUDACC__
+namespace acob200 {
+
+// Philox4x32-10 (Salmon et al., SC'11).
+__device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1,
+                                              uint32_t c2, uint32_t c3,
+                                              uint32_t k0, uint32_t k1,
+                                              uint32_t out[4]) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+// Squared distance in float without contraction: exact for integer
+// coordinates whose differences are below 2896.
+__device__ __forceinline__ float dist2f(float2 a, float2 b) {
+  float dx = __fsub_rn(a.x, b.x);
+  float dy = __fsub_rn(a.y, b.y);
+  return __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+}
+
+// FP64 Euclidean distance, rounded as sqrt(dx*dx + dy*dy) in double.
+__device__ __forceinline__ double dist64(float2 a, float2 b) {
+  double dx = __dsub_rn((double)a.x, (double)b.x);
+  double dy = __dsub_rn((double)a.y, (double)b.y);
+  return __dsqrt_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(kFull, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+__device__ __forceinline__ unsigned long long global_timer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar,
+                                                      uint32_t bytes) {
+  asm volatile(
+      "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+          smem_addr(bar)),
+      "r"(bytes)
+      : "memory");
+}
+
+// 1-D bulk copy global -> shared (TMA engine), completing on an mbarrier.
+// dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src,
+                                         uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n"
+      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: gives up after max_polls polls (returns false).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar,
+                                                  uint32_t parity,
+                                                  uint32_t max_polls) {
+  for (uint32_t i = 0; i < max_polls; ++i) {
+    if (mbar_try_wait(bar, parity)) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ uint8_t ld_cg_u8(const uint8_t *p) {
+  unsigned short v;
+  asm volatile("ld.global.cg.u8 %0, [%1];" : "=h"(v) : "l"(p));
+  return (uint8_t)v;
+}
+
+__device__ __forceinline__ void st_cg_u8(uint8_t *p, uint8_t v) {
+  unsigned short w = v;
+  asm volatile("st.global.cg.u8 [%0], %1;" ::"l"(p), "h"(w) : "memory");
+}
+
+}  // namespace acob200
+#endif

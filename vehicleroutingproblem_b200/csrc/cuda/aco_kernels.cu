@@ -1,0 +1,955 @@
+// aco_kernels.cu -- sm_100a kernels of the ACO-for-CVRP hot path.
+//
+//   k_knn_levels      candidate lists + eta levels, warp per node
+//                     (reference: kernel_build_candidate_lists,
+//                      src/cuda/aco_cuda_kernels.cu:164-214)
+//   k_weights         per-epoch integer weights from the quantized pheromone
+//                     (role of seq_shared_update_scores,
+//                      src/seq/aco_sequential.c:410-442)
+//   k_construct       warp-per-ant route construction with the sequential
+//                     path's rules (src/seq/aco_sequential.c:477-681) over
+//                     candidate tables staged in shared memory by the TMA
+//                     engine (reference kernel: aco_cuda_kernels.cu:447-562)
+//   k_best            iteration best, global best and stop rules on the
+//                     device (src/cuda/aco_cuda.cu:83-126, :331-399)
+//   k_evap_deposit    128-bit streaming evaporation, then the deposit of the
+//                     iteration best and global best by the last block
+//                     (aco_cuda_kernels.cu:145-155, :569-668)
+#include "aco_internal.cuh"
+
+#include <cfloat>
+#include <climits>
+
+namespace acob200 {
+
+// ===========================================================================
+// Candidate lists and eta levels
+// ===========================================================================
+
+__device__ __forceinline__ int level_of(float d2, const float *thr, int J) {
+  int lo = 0, hi = J;  // number of thresholds <= d2
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(thr + mid) <= d2) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Warp-wide k-nearest selection for node i: the k smallest keys
+// (d^2 bits << 32 | j) over j in 1..n, j != i.  Lane t < k ends holding the
+// t-th smallest (~0 when fewer than k exist).  Keys are unique, so the order
+// is total: ascending d^2, ties to the lower j, as the reference's insertion
+// with a strict '<' (aco_cuda_kernels.cu:187-201).
+__device__ unsigned long long warp_knn(const float2 *coords, int n, int k,
+                                       int i, int lane) {
+  const unsigned long long kNone = ~0ull;
+  unsigned long long list = kNone;
+  unsigned long long kth = kNone;
+  const float2 pi = coords[i];
+  for (int base = 1; base <= n; base += 32) {
+    int j = base + lane;
+    unsigned long long key = kNone;
+    if (j <= n && j != i) {
+      float d2 = dist2f(pi, __ldg(coords + j));
+      key = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)j;
+    }
+    unsigned m = __ballot_sync(kFull, key < kth);
+    while (m) {
+      int b = __ffs(m) - 1;
+      m &= m - 1;
+      unsigned long long x = __shfl_sync(kFull, key, b);
+      if (x < kth) {
+        int pos = __popc(__ballot_sync(kFull, lane < k && list < x));
+        unsigned long long up = __shfl_up_sync(kFull, list, 1);
+        if (lane > pos) list = up;
+        else if (lane == pos) list = x;
+        kth = __shfl_sync(kFull, list, k - 1);
+      }
+    }
+  }
+  return list;
+}
+
+__global__ void __launch_bounds__(256) k_knn_levels(
+    const float2 *__restrict__ coords, int n, int k,
+    const float *__restrict__ thr, int J, uint16_t *__restrict__ cand,
+    uint16_t *__restrict__ lvl) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i <= n;
+       i += warps) {
+    unsigned long long key = warp_knn(coords, n, k, i, lane);
+    if (lane < k) {
+      int node = (key == ~0ull) ? 0 : (int)(key & 0xffffffffu);
+      float d2 = __uint_as_float((unsigned)(key >> 32));
+      cand[(size_t)i * k + lane] = (uint16_t)node;
+      lvl[(size_t)i * k + lane] = (uint16_t)(node ? level_of(d2, thr, J) : 0);
+    }
+  }
+}
+
+cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
+                              const float *thr, int J, uint16_t *cand,
+                              uint16_t *lvl, cudaStream_t s) {
+  int rows = n + 1;
+  int blocks = (rows + 7) / 8;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_knn_levels<<<blocks, 256, 0, s>>>(coords, n, k, thr, J, cand, lvl);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Byte fill (pheromone initialisation, kernel_init_tau :131-136)
+// ===========================================================================
+
+__global__ void k_fill_u8(uint8_t *p, unsigned long long count, uint8_t v) {
+  const unsigned long long nvec = count / 16;
+  const uint32_t w = 0x01010101u * v;
+  const uint4 vv = make_uint4(w, w, w, w);
+  uint4 *p4 = reinterpret_cast<uint4 *>(p);
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+       i < nvec; i += stride)
+    p4[i] = vv;
+  if (blockIdx.x == 0) {
+    for (unsigned long long i = nvec * 16 + threadIdx.x; i < count; i += blockDim.x) p[i] = v;
+  }
+}
+
+cudaError_t launch_fill_u8(uint8_t *p, unsigned long long count, uint8_t v,
+                           cudaStream_t s) {
+  unsigned long long nvec = count / 16;
+  unsigned long long blocks = (nvec + 255) / 256;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_fill_u8<<<(unsigned)blocks, 256, 0, s>>>(p, count, v);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Per-epoch weights
+// ===========================================================================
+
+__global__ void __launch_bounds__(256) k_weights(InstanceView iv,
+                                                 PheromoneView pv,
+                                                 EpochTables et,
+                                                 DevState *st) {
+  if (st) {
+    int stop = *(volatile int *)&st->stop_flags;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->skip = stop ? 1 : 0;
+      if (!stop && st->start_ns == 0ull) st->start_ns = global_timer_ns();
+    }
+    if (stop) return;
+  }
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int k = iv.k;
+  const size_t stride = (size_t)iv.n + 1;
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i <= iv.n;
+       i += warps) {
+    int c = 0;
+    int e = INT_MIN;
+    if (lane < k) {
+      c = iv.cand[(size_t)i * k + lane];
+      if (c > 0) {
+        uint8_t q = pv.tau[(size_t)i * stride + c];
+        e = __ldg(et.A + q) - (int)iv.lvl[(size_t)i * k + lane];
+      }
+    }
+    int emax = __reduce_max_sync(kFull, e);
+    if (lane < k) {
+      uint32_t w = 0u;
+      uint8_t rel = (uint8_t)kRelMax;
+      if (c > 0) {
+        int r = emax - e;
+        if (r > kRelMax) r = kRelMax;
+        rel = (uint8_t)r;
+        w = __ldg(et.lut + r);
+      }
+      et.w[(size_t)i * k + lane] = w;
+      et.rel[(size_t)i * k + lane] = rel;
+    }
+  }
+}
+
+cudaError_t launch_weights(const InstanceView &iv, const PheromoneView &pv,
+                           const EpochTables &et, DevState *st,
+                           cudaStream_t s) {
+  int rows = iv.n + 1;
+  int blocks = (rows + 7) / 8;
+  if (blocks > 148 * 8) blocks = 148 * 8;
+  k_weights<<<blocks, 256, 0, s>>>(iv, pv, et, st);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Construction
+// ===========================================================================
+
+// Per-lane Philox block of the current 128-draw batch.  Draw d of an ant is
+// word d%4 of Philox({d/4, ant, epoch, stream}, {seed, kDrawKey1}) >> 8; lane
+// L of batch b holds block 32 b + L.
+struct DrawBuf {
+  uint32_t r[4];
+  uint32_t d;
+};
+
+__device__ __forceinline__ void draw_fill(DrawBuf &db, uint32_t seed,
+                                          uint32_t epoch, uint32_t ant,
+                                          uint32_t stream, int lane) {
+  uint32_t blk = ((db.d >> 7) << 5) + (uint32_t)lane;
+  philox4x32_10(blk, ant, epoch, stream, seed, kDrawKey1, db.r);
+}
+
+__device__ __forceinline__ uint32_t draw_peek(const DrawBuf &db) {
+  uint32_t w = db.d & 3u;
+  uint32_t v = (w == 0) ? db.r[0] : (w == 1) ? db.r[1] : (w == 2) ? db.r[2] : db.r[3];
+  return __shfl_sync(kFull, v, (db.d >> 2) & 31u) >> (32 - kDrawBits);
+}
+
+template <int L, bool UNIT>
+struct Tables {
+  const uint16_t *cand;
+  const uint32_t *w;
+  const uint8_t *rel;
+  const uint32_t *lut;
+  const float2 *coords;
+  const int *dem;
+
+  __device__ __forceinline__ uint32_t weight(size_t idx) const {
+    if (L == kLayoutSmemPacked) return lut[rel[idx]];
+    return w[idx];
+  }
+  __device__ __forceinline__ float2 coord(int node) const {
+    if (L == kLayoutGlobal) return __ldg(coords + node);
+    return coords[node];
+  }
+  __device__ __forceinline__ long long demand(int node) const {
+    if (UNIT) return 1;
+    if (L == kLayoutGlobal) return (long long)__ldg(dem + node);
+    return (long long)dem[node];
+  }
+};
+
+// Nearest unvisited customer that fits (find_nearest_unvisited,
+// src/seq/aco_sequential.c:477-493: strict '<' over ascending nodes, so the
+// lowest index wins ties).  0 if none.
+template <int L, bool UNIT>
+__device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
+                                                 const uint32_t *vis, int vw,
+                                                 float2 pc, long long load,
+                                                 long long cap, int lane) {
+  uint32_t best_h = 0xffffffffu, best_n = 0xffffffffu;
+  for (int wi = lane; wi < vw; wi += 32) {
+    uint32_t fr = ~vis[wi];
+    while (fr) {
+      int b = __ffs(fr) - 1;
+      fr &= fr - 1;
+      int node = (wi << 5) + b;
+      if (!UNIT && load + tb.demand(node) > cap) continue;
+      uint32_t h = __float_as_uint(dist2f(pc, tb.coord(node)));
+      if (h < best_h) {
+        best_h = h;
+        best_n = (uint32_t)node;
+      }
+    }
+  }
+  uint32_t mh = __reduce_min_sync(kFull, best_h);
+  uint32_t mn = __reduce_min_sync(kFull, best_h == mh ? best_n : 0xffffffffu);
+  return (mh == 0xffffffffu) ? 0 : (int)mn;
+}
+
+struct ConstructArgs {
+  InstanceView iv;
+  EpochTables et;
+  AntBuffers ab;
+  SmemPlan plan;
+  DevState *st;
+  uint32_t seed;
+  uint32_t epoch;
+  uint32_t stream;
+  int use_state_epoch;  // 1: epoch number = st->epoch (graph replays)
+};
+
+// One ant, one warp.  Rules of build_ant_solution
+// (src/seq/aco_sequential.c:616-681) with the demand extension:
+//   vehicle v extends while remaining > 0, remaining demand > (K-v-1) Q and
+//   load < Q; the next customer is drawn by roulette over the eligible
+//   candidates (unvisited, load + d <= Q), else the nearest eligible one;
+//   customers left over are added by the backward repair pass.
+template <int L, bool UNIT>
+__device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
+                          uint32_t *vis, int ant, uint32_t epoch, int lane) {
+  const InstanceView &iv = a.iv;
+  const int k = iv.k, K = iv.K, R = iv.route_stride, vw = a.plan.vis_words;
+  const long long cap = iv.cap;
+  int *route = a.ab.routes + (size_t)ant * R;
+  int *lens = a.ab.lens + (size_t)ant * K;
+  long long *loads = a.ab.loads + (size_t)ant * K;
+
+  DrawBuf db;
+  db.d = 0;
+  draw_fill(db, a.seed, epoch, (uint32_t)ant, a.stream, lane);
+  uint32_t r_next = draw_peek(db);
+
+  long long remaining = iv.n;
+  long long rem_dem = iv.total_demand;
+  double cost = 0.0;
+  int pos = 0;
+  const float2 depot = tb.coord(0);
+
+  for (int v = 0; v < K; ++v) {
+    const int start = pos;
+    if (lane == 0) route[pos] = 0;
+    ++pos;
+    int cur = 0;
+    float2 pc = depot;
+    long long load = 0;
+    const long long future = (long long)(K - v - 1) * cap;
+    while (remaining > 0 && rem_dem > future && load < cap) {
+      const size_t base = (size_t)cur * k;
+      int c = 0;
+      uint32_t w = 0u;
+      if (lane < k) {
+        c = tb.cand[base + lane];
+        w = tb.weight(base + lane);
+      }
+      bool ok = ((vis[c >> 5] >> (c & 31)) & 1u) == 0u;
+      if (!UNIT) ok = ok && (load + tb.demand(c) <= cap);
+      const uint32_t wv = ok ? w : 0u;
+      const uint32_t cum = warp_incl_scan(wv, lane);
+      const uint32_t denom = __shfl_sync(kFull, cum, 31);
+      int next;
+      if (denom != 0u) {
+        const unsigned long long T = (unsigned long long)r_next * denom;
+        const bool sel = (wv != 0u) && (((unsigned long long)cum << kDrawBits) >= T);
+        const unsigned m = __ballot_sync(kFull, sel);
+        // m is never empty: at the last eligible lane cum = denom and
+        // r < 2^24.  The guard keeps the shuffle source in range regardless.
+        next = m ? __shfl_sync(kFull, c, __ffs(m) - 1) : 0;
+        ++db.d;
+        if ((db.d & 127u) == 0u) draw_fill(db, a.seed, epoch, (uint32_t)ant, a.stream, lane);
+        r_next = draw_peek(db);
+        if (next <= 0) break;
+      } else {
+        next = nearest_unvisited<L, UNIT>(tb, vis, vw, pc, load, cap, lane);
+        if (next <= 0) break;
+      }
+      const float2 pn = tb.coord(next);
+      if (lane == 0) {
+        route[pos] = next;
+        vis[next >> 5] |= 1u << (next & 31);
+        cost = __dadd_rn(cost, dist64(pc, pn));
+      }
+      __syncwarp();
+      ++pos;
+      const long long dn = tb.demand(next);
+      load += dn;
+      --remaining;
+      rem_dem -= dn;
+      cur = next;
+      pc = pn;
+    }
+    if (lane == 0) {
+      route[pos] = 0;
+      cost = __dadd_rn(cost, dist64(pc, depot));
+      lens[v] = pos + 1 - start;
+      loads[v] = load;
+    }
+    ++pos;
+  }
+
+  if (remaining > 0) {
+    // Backward repair (aco_sequential.c:659-680): from the last vehicle down,
+    // reopen the route and append the nearest eligible customers.
+    __syncwarp();
+    int *rep = a.ab.rep + (size_t)ant * iv.n;
+    int *repc = a.ab.repc + (size_t)ant * K;
+    for (int v = lane; v < K; v += 32) repc[v] = 0;
+    __syncwarp();
+    int nrep = 0;
+    int off_end = pos;
+    for (int v = K - 1; v >= 0 && remaining > 0; --v) {
+      const int len_v = lens[v];
+      off_end -= len_v;
+      int cur = route[off_end + len_v - 2];
+      float2 pc = tb.coord(cur);
+      long long load = loads[v];
+      int cnt = 0;
+      while (remaining > 0 && load < cap) {
+        int next = nearest_unvisited<L, UNIT>(tb, vis, vw, pc, load, cap, lane);
+        if (next <= 0) break;
+        if (lane == 0) {
+          rep[nrep + cnt] = next;
+          vis[next >> 5] |= 1u << (next & 31);
+        }
+        __syncwarp();
+        ++cnt;
+        load += tb.demand(next);
+        --remaining;
+        cur = next;
+        pc = tb.coord(next);
+      }
+      if (lane == 0) repc[v] = cnt;
+      nrep += cnt;
+    }
+    __syncwarp();
+    if (lane == 0 && nrep > 0) {
+      // Re-lay the compact routes with each vehicle's additions appended
+      // before its closing depot; vehicles are moved right, last first.
+      int off_total = pos;
+      int add_after = 0;  // additions of vehicles > v (stored first)
+      int shift = nrep;   // additions of vehicles <= v
+      for (int v = K - 1; v >= 0; --v) {
+        const int len_v = lens[v];
+        off_total -= len_v;
+        const int cnt = repc[v];
+        shift -= cnt;  // now: additions of vehicles < v
+        const int old_off = off_total, new_off = off_total + shift;
+        const int main_len = len_v - 1;
+        for (int t = main_len - 1; t >= 0; --t) route[new_off + t] = route[old_off + t];
+        for (int j = 0; j < cnt; ++j) route[new_off + main_len + j] = rep[add_after + j];
+        route[new_off + main_len + cnt] = 0;
+        lens[v] = len_v + cnt;
+        add_after += cnt;
+      }
+      pos += nrep;
+      // FP64 cost in final route order (solution_cost, solution.c:126-137).
+      cost = 0.0;
+      int off = 0;
+      for (int v = 0; v < K; ++v) {
+        for (int t = 1; t < lens[v]; ++t)
+          cost = __dadd_rn(cost, dist64(tb.coord(route[off + t - 1]), tb.coord(route[off + t])));
+        off += lens[v];
+      }
+    }
+    __syncwarp();
+  }
+
+  if (lane == 0) {
+    a.ab.cost[ant] = cost;
+    a.ab.feasible[ant] = (remaining == 0) ? 1 : 0;
+    a.ab.steps[ant] = pos - K;
+    a.ab.draws[ant] = db.d;
+  }
+}
+
+template <int L, bool UNIT>
+__global__ void __launch_bounds__(1024, 1) k_construct(ConstructArgs a) {
+  if (a.st && *(volatile int *)&a.st->skip) return;
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const SmemPlan &pl = a.plan;
+  const InstanceView &iv = a.iv;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+
+  Tables<L, UNIT> tb;
+  if (L == kLayoutGlobal) {
+    tb.cand = iv.cand;
+    tb.w = a.et.w;
+    tb.rel = nullptr;
+    tb.lut = nullptr;
+    tb.coords = iv.coords;
+    tb.dem = iv.demand;
+  } else {
+    tb.cand = reinterpret_cast<const uint16_t *>(smem + pl.off_cand);
+    tb.w = reinterpret_cast<const uint32_t *>(smem + pl.off_w);
+    tb.rel = reinterpret_cast<const uint8_t *>(smem + pl.off_w);
+    tb.lut = reinterpret_cast<const uint32_t *>(smem + pl.off_lut);
+    tb.coords = reinterpret_cast<const float2 *>(smem + pl.off_coords);
+    tb.dem = reinterpret_cast<const int *>(smem + pl.off_dem);
+    if (threadIdx.x == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t total = pl.bytes_cand + pl.bytes_w + pl.bytes_coords + (UNIT ? 0u : pl.bytes_dem);
+      mbar_arrive_expect_tx(bar, total);
+      const uint32_t kChunk = 32768u;
+      auto issue = [&](unsigned char *dst, const void *src, uint32_t bytes) {
+        const unsigned char *s = reinterpret_cast<const unsigned char *>(src);
+        for (uint32_t o = 0; o < bytes; o += kChunk) {
+          uint32_t b = bytes - o < kChunk ? bytes - o : kChunk;
+          bulk_g2s(dst + o, s + o, b, bar);
+        }
+      };
+      issue(smem + pl.off_cand, iv.cand, pl.bytes_cand);
+      if (L == kLayoutSmemPacked) issue(smem + pl.off_w, a.et.rel, pl.bytes_w);
+      else issue(smem + pl.off_w, a.et.w, pl.bytes_w);
+      issue(smem + pl.off_coords, iv.coords, pl.bytes_coords);
+      if (!UNIT) issue(smem + pl.off_dem, iv.demand, pl.bytes_dem);
+    }
+    if (L == kLayoutSmemPacked) {
+      uint32_t *lut = reinterpret_cast<uint32_t *>(smem + pl.off_lut);
+      for (int r = threadIdx.x; r < 256; r += blockDim.x) lut[r] = __ldg(a.et.lut + r);
+    }
+  }
+
+  // Visited bitmap of this warp's ant: the depot and the bits past node n
+  // are set so that scans see customers only.
+  uint32_t *vis = reinterpret_cast<uint32_t *>(smem + pl.off_vis) + (size_t)warp * pl.vis_words;
+  for (int wi = lane; wi < pl.vis_words; wi += 32) {
+    uint32_t word = 0u;
+    int lo = wi << 5;
+    if (lo == 0) word |= 1u;
+    int valid = iv.n + 1 - lo;  // nodes lo..n in this word
+    if (valid < 32) word |= (valid <= 0) ? 0xffffffffu : (0xffffffffu << valid);
+    vis[wi] = word;
+  }
+  if (L == kLayoutSmemPacked) __syncthreads();
+  __syncwarp();
+
+  if (L != kLayoutGlobal) {
+    if (!mbar_wait_bounded(bar, 0, 1u << 22)) {
+      if (lane == 0 && a.st) atomicOr(&a.st->error, kErrStageTimeout);
+      return;
+    }
+  }
+
+  const int ant = blockIdx.x * pl.wpb + warp;
+  if (ant >= iv.m) return;
+  const uint32_t epoch = a.use_state_epoch ? (uint32_t)a.st->epoch : a.epoch;
+  build_ant<L, UNIT>(a, tb, vis, ant, epoch, lane);
+}
+
+static int g_max_smem = 0;
+
+int construct_max_smem() {
+  if (g_max_smem == 0) {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    g_max_smem = v;
+  }
+  return g_max_smem;
+}
+
+static uint32_t pad16(size_t b) { return (uint32_t)((b + 15) & ~size_t(15)); }
+
+SmemPlan plan_construct(const InstanceView &iv, int layout, int num_sms,
+                        int max_smem) {
+  SmemPlan p = {};
+  const size_t rows = (size_t)iv.n + 1;
+  p.vis_words = (int)((rows + 31) / 32);
+  int wpb = (iv.m + num_sms - 1) / num_sms;
+  if (wpb < 1) wpb = 1;
+  if (wpb > 32) wpb = 32;
+  p.wpb = wpb;
+  p.bytes_cand = pad16(rows * iv.k * sizeof(uint16_t));
+  p.bytes_coords = pad16(rows * sizeof(float2));
+  p.bytes_dem = iv.unit ? 0u : pad16(rows * sizeof(int));
+  const uint32_t vis_bytes = (uint32_t)wpb * p.vis_words * 4u;
+  auto finish = [&](int lay) {
+    p.layout = lay;
+    uint32_t off = 16;  // mbarrier
+    if (lay == kLayoutGlobal) {
+      p.bytes_cand = p.bytes_w = p.bytes_coords = p.bytes_dem = 0;
+      p.off_cand = p.off_w = p.off_coords = p.off_dem = p.off_lut = off;
+    } else {
+      p.bytes_w = (lay == kLayoutSmemPacked) ? pad16(rows * iv.k) : pad16(rows * iv.k * 4);
+      p.off_cand = off; off += p.bytes_cand;
+      p.off_w = off; off += p.bytes_w;
+      p.off_coords = off; off += p.bytes_coords;
+      p.off_dem = off; off += p.bytes_dem;
+      p.off_lut = off; off += (lay == kLayoutSmemPacked) ? 1024u : 0u;
+    }
+    p.off_vis = off;
+    off += vis_bytes;
+    p.total = off;
+  };
+  if (layout >= 0) {
+    finish(layout);
+    return p;
+  }
+  finish(kLayoutSmemWeights);
+  if ((int)p.total <= max_smem) return p;
+  finish(kLayoutSmemPacked);
+  if ((int)p.total <= max_smem) return p;
+  finish(kLayoutGlobal);
+  return p;
+}
+
+template <int L, bool UNIT>
+static cudaError_t configure_t() {
+  return cudaFuncSetAttribute(k_construct<L, UNIT>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              construct_max_smem());
+}
+
+// Opts every construct instantiation into the full shared-memory carve-out;
+// called once per device before any launch or graph capture.
+cudaError_t prepare_construct_kernels() {
+  cudaError_t e = configure_t<kLayoutSmemWeights, false>();
+  if (e == cudaSuccess) e = configure_t<kLayoutSmemWeights, true>();
+  if (e == cudaSuccess) e = configure_t<kLayoutSmemPacked, false>();
+  if (e == cudaSuccess) e = configure_t<kLayoutSmemPacked, true>();
+  if (e == cudaSuccess) e = configure_t<kLayoutGlobal, false>();
+  if (e == cudaSuccess) e = configure_t<kLayoutGlobal, true>();
+  return e;
+}
+
+template <int L, bool UNIT>
+static cudaError_t launch_construct_t(const ConstructArgs &a, cudaStream_t s) {
+  const int grid = (a.iv.m + a.plan.wpb - 1) / a.plan.wpb;
+  k_construct<L, UNIT><<<grid, a.plan.wpb * 32, a.plan.total, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_construct(const InstanceView &iv, const EpochTables &et,
+                             const AntBuffers &ab, const SmemPlan &plan,
+                             DevState *st, uint32_t seed, uint32_t epoch,
+                             uint32_t stream_id, int use_state_epoch,
+                             cudaStream_t s) {
+  ConstructArgs a;
+  a.iv = iv;
+  a.et = et;
+  a.ab = ab;
+  a.plan = plan;
+  a.st = st;
+  a.seed = seed;
+  a.epoch = epoch;
+  a.stream = stream_id;
+  a.use_state_epoch = use_state_epoch;
+  if ((int)plan.total > construct_max_smem()) return cudaErrorInvalidValue;
+  switch (plan.layout * 2 + (iv.unit ? 1 : 0)) {
+    case 0: return launch_construct_t<kLayoutSmemWeights, false>(a, s);
+    case 1: return launch_construct_t<kLayoutSmemWeights, true>(a, s);
+    case 2: return launch_construct_t<kLayoutSmemPacked, false>(a, s);
+    case 3: return launch_construct_t<kLayoutSmemPacked, true>(a, s);
+    case 4: return launch_construct_t<kLayoutGlobal, false>(a, s);
+    case 5: return launch_construct_t<kLayoutGlobal, true>(a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// ===========================================================================
+// Iteration best, global best and stop rules
+// ===========================================================================
+
+// is_significant_improvement, src/cuda/aco_cuda.cu:83-94.
+__device__ __forceinline__ bool significant(double prev, double next,
+                                            double min_rel) {
+  if (prev >= DBL_MAX || next >= DBL_MAX) return next < prev;
+  if (next >= __dsub_rn(prev, 1e-9)) return false;
+  double gain = __dsub_rn(prev, next);
+  double rel = __ddiv_rn(gain, fmax(prev, 1e-9));
+  return __dadd_rn(rel, 1e-9) >= min_rel;
+}
+
+__global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
+                                               DevState *st, int *gbest_nodes,
+                                               int *gbest_lens, EpochRec *log) {
+  if (*(volatile int *)&st->skip) return;
+  __shared__ double s_cost[32];
+  __shared__ int s_ant[32];
+  __shared__ unsigned long long s_steps[32];
+  __shared__ int s_improved, s_best;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double bc = DBL_MAX;
+  int ba = INT_MAX;
+  unsigned long long steps = 0;
+  for (int i = threadIdx.x; i < iv.m; i += blockDim.x) {
+    steps += (unsigned long long)ab.steps[i];
+    if (ab.feasible[i]) {
+      double c = ab.cost[i];
+      if (ba == INT_MAX || c < bc) {  // ascending i: first minimum kept
+        bc = c;
+        ba = i;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double oc = __shfl_down_sync(kFull, bc, o);
+    int oa = __shfl_down_sync(kFull, ba, o);
+    steps += __shfl_down_sync(kFull, steps, o);
+    if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
+      bc = oc;
+      ba = oa;
+    }
+  }
+  if (lane == 0) {
+    s_cost[warp] = bc;
+    s_ant[warp] = ba;
+    s_steps[warp] = steps;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    const int nw = blockDim.x >> 5;
+    bc = (lane < nw) ? s_cost[lane] : DBL_MAX;
+    ba = (lane < nw) ? s_ant[lane] : INT_MAX;
+    steps = (lane < nw) ? s_steps[lane] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      double oc = __shfl_down_sync(kFull, bc, o);
+      int oa = __shfl_down_sync(kFull, ba, o);
+      steps += __shfl_down_sync(kFull, steps, o);
+      if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
+        bc = oc;
+        ba = oa;
+      }
+    }
+    if (lane == 0) {
+      // Epoch bookkeeping of src/cuda/aco_cuda.cu:349-399 and the stop
+      // rules checked at the start of the next epoch (:333-339).
+      const bool found = (ba != INT_MAX);
+      int improved = 0;
+      st->found = found ? 1 : 0;
+      st->total_steps += steps;
+      if (found) {
+        st->iter_best = bc;
+        st->best_ant = ba;
+        if (bc < st->global_best) {
+          improved = 1;
+          if (significant(st->global_best, bc, st->min_rel)) st->iter_since_best = 0;
+          else st->iter_since_best += 1;
+          st->global_best = bc;
+        } else {
+          st->iter_since_best += 1;
+        }
+        st->dep_iter = __fdiv_rn(0.3f * st->Qs, (float)bc);
+        st->dep_global = __fdiv_rn(0.7f * st->Qs, (float)st->global_best);
+      } else {
+        st->iter_since_best += 1;
+      }
+      st->improved = improved;
+      st->epoch += 1;
+      const unsigned long long now = global_timer_ns();
+      const unsigned long long elapsed = now > st->start_ns ? now - st->start_ns : 0ull;
+      EpochRec rec;
+      rec.epoch = st->epoch;
+      rec.iter_since_best = st->iter_since_best;
+      rec.improved = improved;
+      rec.found = found ? 1 : 0;
+      rec.global_best = st->global_best;
+      rec.elapsed_ns = elapsed;
+      log[st->log_count % kLogCap] = rec;
+      st->log_count += 1;
+      int flags = st->stop_flags;
+      if (st->stagnation > 0 && st->iter_since_best >= st->stagnation) flags |= kStopStagnation;
+      if (st->fixed_epochs > 0 && st->epoch >= st->fixed_epochs) flags |= kStopFixed;
+      if (st->timeout_ns > 0ull && elapsed > st->timeout_ns) flags |= kStopTimeout;
+      if (st->run_limit > 0 && st->epoch >= st->run_limit) flags |= kStopRunLimit;
+      st->stop_flags = flags;
+      s_improved = improved;
+      s_best = ba;
+    }
+  }
+  __syncthreads();
+  if (s_improved) {
+    // New global best: keep a copy (the reference copies it to the host and
+    // uploads a flat buffer, aco_cuda.cu:367-380).
+    const int *src = ab.routes + (size_t)s_best * iv.route_stride;
+    const int *sl = ab.lens + (size_t)s_best * iv.K;
+    int total = 0;
+    for (int v = 0; v < iv.K; ++v) total += sl[v];
+    for (int t = threadIdx.x; t < total; t += blockDim.x) gbest_nodes[t] = src[t];
+    for (int v = threadIdx.x; v < iv.K; v += blockDim.x) gbest_lens[v] = sl[v];
+  }
+}
+
+cudaError_t launch_best(const InstanceView &iv, const AntBuffers &ab,
+                        DevState *st, int *gbest_nodes, int *gbest_lens,
+                        EpochRec *log, cudaStream_t s) {
+  k_best<<<1, 1024, 0, s>>>(iv, ab, st, gbest_nodes, gbest_lens, log);
+  return cudaGetLastError();
+}
+
+__global__ void k_set_run_limit(DevState *st, int limit) {
+  st->run_limit = limit;
+  st->stop_flags &= ~kStopRunLimit;
+  if (limit > 0 && st->epoch >= limit) st->stop_flags |= kStopRunLimit;
+}
+
+cudaError_t launch_set_run_limit(DevState *st, int limit, cudaStream_t s) {
+  k_set_run_limit<<<1, 1, 0, s>>>(st, limit);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Evaporation + deposit
+// ===========================================================================
+
+// quantize_tau / dequantize_tau of the reference (aco_cuda_kernels.cu:25-45),
+// the same expressions so that the device math rounds identically.
+__device__ __forceinline__ float dequant(uint8_t q, float log_min, float log_step) {
+  return expf((float)q * log_step + log_min);
+}
+
+__device__ __forceinline__ uint8_t quant(float tau, float log_min,
+                                         float log_step, uint8_t q_min,
+                                         uint8_t q_max) {
+  if (tau <= 0.0f) return q_min;
+  float log_t = logf(tau);
+  float q_f = (log_t - log_min) / log_step;
+  if (q_f <= (float)q_min) return q_min;
+  if (q_f >= (float)q_max) return q_max;
+  return (uint8_t)roundf(q_f);
+}
+
+// One arc (u, c): new = quantize(dequantize(tau[u][c]) + dep), max-ed into
+// tau[u][c] and tau[c][u] (aco_cuda_kernels.cu:614-623).  The caller
+// guarantees that no other thread touches these two cells concurrently.
+__device__ __forceinline__ void deposit_arc(const PheromoneView &pv,
+                                            size_t stride, int u, int c,
+                                            float dep) {
+  uint8_t *fwd = pv.tau + (size_t)u * stride + c;
+  uint8_t *rev = pv.tau + (size_t)c * stride + u;
+  const uint8_t old = ld_cg_u8(fwd);
+  const uint8_t nq = quant(dequant(old, pv.log_min, pv.log_step) + dep,
+                           pv.log_min, pv.log_step, pv.q_min, pv.q_max);
+  if (nq > old) st_cg_u8(fwd, nq);
+  const uint8_t oldr = ld_cg_u8(rev);
+  if (nq > oldr) st_cg_u8(rev, nq);
+}
+
+// Deposit of one solution by one block.  Arcs of different routes touch
+// different cells, except the depot loop (0,0) of empty routes, so the arcs
+// of routes of >= 4 nodes are dealt round-robin over the threads; a
+// one-customer route [0 a 0] (whose two arcs share the cells {0,a}) is
+// walked by one thread, and all empty routes by thread 0 in vehicle order.
+__device__ void deposit_solution(const PheromoneView &pv, size_t stride,
+                                 const int *nodes, const int *lens, int K,
+                                 float dep) {
+  const int bd = (int)blockDim.x, tid = (int)threadIdx.x;
+  int off = 0, base = 0;  // node offset and arc count before route v
+  for (int v = 0; v < K; ++v) {
+    const int len = lens[v];
+    const int owner = base % bd;
+    if (len >= 4) {
+      for (int t = (tid - owner + bd) % bd; t < len - 1; t += bd)
+        deposit_arc(pv, stride, nodes[off + t], nodes[off + t + 1], dep);
+    } else if (len == 3) {
+      if (tid == owner) {
+        deposit_arc(pv, stride, nodes[off], nodes[off + 1], dep);
+        deposit_arc(pv, stride, nodes[off + 1], nodes[off + 2], dep);
+      }
+    } else if (len == 2) {
+      if (tid == 0) deposit_arc(pv, stride, nodes[off], nodes[off + 1], dep);
+    }
+    off += len;
+    base += len > 1 ? len - 1 : 0;
+  }
+}
+
+__device__ __forceinline__ uint32_t evap4(uint32_t x, uint32_t floor4,
+                                          uint32_t delta4) {
+  return __vsub4(__vmaxu4(x, floor4), delta4);
+}
+
+struct EvapArgs {
+  InstanceView iv;
+  PheromoneView pv;
+  AntBuffers ab;
+  DevState *st;
+  const int *gbest_nodes;
+  const int *gbest_lens;
+  unsigned int *counter;
+  int best_ant;          // used when st == nullptr
+  float dep_iter, dep_global;
+};
+
+__global__ void __launch_bounds__(512) k_evap_deposit(EvapArgs a) {
+  if (a.st) {
+    if (*(volatile int *)&a.st->skip || !*(volatile int *)&a.st->found) return;
+  }
+  const PheromoneView &pv = a.pv;
+  // q > q_min + delta ? q - delta : q_min  ==  max(q, q_min + delta) - delta
+  const int fl = (int)pv.q_min + (int)pv.delta;
+  const bool sat_all = fl > 255;
+  const uint32_t floor4 = 0x01010101u * (uint32_t)(sat_all ? 0 : fl);
+  const uint32_t delta4 = 0x01010101u * (uint32_t)pv.delta;
+  const uint32_t qmin4 = 0x01010101u * (uint32_t)pv.q_min;
+  const unsigned long long nvec = pv.total / 16;
+  uint4 *p4 = reinterpret_cast<uint4 *>(pv.tau);
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+       i < nvec; i += stride) {
+    uint4 v = p4[i];
+    if (sat_all) {
+      v = make_uint4(qmin4, qmin4, qmin4, qmin4);
+    } else {
+      v.x = evap4(v.x, floor4, delta4);
+      v.y = evap4(v.y, floor4, delta4);
+      v.z = evap4(v.z, floor4, delta4);
+      v.w = evap4(v.w, floor4, delta4);
+    }
+    p4[i] = v;
+  }
+  if (blockIdx.x == 0) {
+    for (unsigned long long i = nvec * 16 + threadIdx.x; i < pv.total; i += blockDim.x) {
+      uint8_t q = pv.tau[i];
+      pv.tau[i] = ((int)q > fl) ? (uint8_t)(q - pv.delta) : pv.q_min;
+    }
+  }
+  // The last block to finish the sweep deposits (threadfence reduction).
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned ticket = atomicAdd(a.counter, 1u);
+    s_last = (ticket == gridDim.x - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const size_t stride_n = (size_t)a.iv.n + 1;
+  const int best = a.st ? a.st->best_ant : a.best_ant;
+  const float dep_i = a.st ? a.st->dep_iter : a.dep_iter;
+  const float dep_g = a.st ? a.st->dep_global : a.dep_global;
+  deposit_solution(pv, stride_n, a.ab.routes + (size_t)best * a.iv.route_stride,
+                   a.ab.lens + (size_t)best * a.iv.K, a.iv.K, dep_i);
+  __syncthreads();
+  if (a.gbest_nodes) {
+    deposit_solution(pv, stride_n, a.gbest_nodes, a.gbest_lens, a.iv.K, dep_g);
+  }
+  if (threadIdx.x == 0) *a.counter = 0u;
+}
+
+cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
+                                const AntBuffers &ab, DevState *st,
+                                const int *gbest_nodes, const int *gbest_lens,
+                                unsigned int *counter, int grid,
+                                cudaStream_t s) {
+  EvapArgs a;
+  a.iv = iv;
+  a.pv = pv;
+  a.ab = ab;
+  a.st = st;
+  a.gbest_nodes = gbest_nodes;
+  a.gbest_lens = gbest_lens;
+  a.counter = counter;
+  a.best_ant = 0;
+  a.dep_iter = a.dep_global = 0.0f;
+  k_evap_deposit<<<grid, 512, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// Test-hook variant with explicit best ant and amounts (no device state).
+cudaError_t launch_evap_deposit_explicit(const InstanceView &iv,
+                                         const PheromoneView &pv,
+                                         const AntBuffers &ab, int best_ant,
+                                         float dep_iter,
+                                         const int *gbest_nodes,
+                                         const int *gbest_lens,
+                                         float dep_global,
+                                         unsigned int *counter, int grid,
+                                         cudaStream_t s) {
+  EvapArgs a;
+  a.iv = iv;
+  a.pv = pv;
+  a.ab = ab;
+  a.st = nullptr;
+  a.gbest_nodes = gbest_nodes;
+  a.gbest_lens = gbest_lens;
+  a.counter = counter;
+  a.best_ant = best_ant;
+  a.dep_iter = dep_iter;
+  a.dep_global = dep_global;
+  k_evap_deposit<<<grid, 512, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace acob200

@@ -79,7 +79,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         return self
 
@@ -206,7 +206,7 @@ def run_reference_arm(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=8)
@@ -228,7 +228,11 @@ def main():
 
     inst = I.workload_n1000()
     n, K, m, k = inst.n, inst.vehicles, WORKLOAD["ants"], WORKLOAD["cand_k"]
-    stream = torch.cuda.current_stream()
+    # A dedicated stream (the default stream's handle is 0, which the C ABI
+    # reads as "use your own stream"): the library's kernels, the L2 flush and
+    # the timing events all go to it.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx = _native.Context(local)
     ctx.set_stream(stream.cuda_stream)
     ctx.setup_instance(inst, ants=m, cand_k=k, seed=1234 + 7919 * rank)
@@ -244,6 +248,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
+        time.sleep(0.5)  # let the sampler start before the timed region
         wall0 = time.perf_counter()
         for i in range(args.steps):
             flush.fill_(i & 0xff)

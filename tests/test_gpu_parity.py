@@ -38,7 +38,16 @@ CASES = {
     "n1000_c2": (I.workload_n1000, 32, 256),
     "n1000_unit": (lambda: I.workload_n1000().unit_twin(), 32, 96),
     "c2000_demand": (lambda: I.clustered_instance(2000, 16, 603), 32, 64),
+    # n >= 2048: visited bitmap in shared memory, rows read from global memory
+    "u3000_demand": (lambda: I.uniform_instance(3000, 24, 604), 32, 32),
+    # K > 4096 routes of one or two customers: the deposit's unstaged path
+    "many_vehicles": (lambda: I.Instance("mv", *_many_vehicles()), 8, 8),
 }
+
+
+def _many_vehicles():
+    base = I.uniform_instance(5000, 4200, 605).unit_twin()
+    return base.x, base.y, base.demand, 4200, 2
 
 
 def make_ctx(inst, k, m, seed=1234, **kw):
@@ -120,7 +129,8 @@ def check_construct(O, inst, ctx, seed, epoch, tau, ants=None):
 
 
 @pytest.mark.parametrize("name", ["smoke", "u200_unit", "small_c1", "u300_demand", "n1000_c2",
-                                  "n1000_unit", "c2000_demand"])
+                                  "n1000_unit", "c2000_demand", "u3000_demand",
+                                  "many_vehicles"])
 def test_construct_matches_oracle(oracle_mod, name):
     factory, k, m = CASES[name]
     inst = factory()
@@ -197,7 +207,7 @@ def _compact_to_flat(nodes, lens, n):
     return flat
 
 
-@pytest.mark.parametrize("name", ["u200_unit", "n1000_c2"])
+@pytest.mark.parametrize("name", ["u200_unit", "n1000_c2", "many_vehicles"])
 def test_evaporate_deposit(oracle_mod, name):
     O = oracle_mod
     factory, k, m = CASES[name]

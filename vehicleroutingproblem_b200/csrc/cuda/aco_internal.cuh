@@ -82,10 +82,11 @@ struct DevState {
 
 // Byte offsets of the construct kernel's dynamic shared memory.
 struct SmemPlan {
-  uint32_t off_cand, off_w, off_coords, off_dem, off_lut, off_vis;
+  uint32_t off_cand, off_w, off_coords, off_dem, off_lut, off_draw, off_vis;
   uint32_t bytes_cand, bytes_w, bytes_coords, bytes_dem;
   uint32_t total;
   int vis_words;           // 32-bit words per ant bitmap
+  int vreg;                // bitmap words per lane held in registers (0: smem)
   int wpb;                 // warps (ants) per block
   int layout;
 };
@@ -95,6 +96,7 @@ struct InstanceView {
   long long cap;
   long long total_demand;
   int unit;                // 1: every customer has demand 1
+  int max_demand;          // largest customer demand
   int route_stride;        // n + 2K
   const float2 *coords;    // [n+1]
   const int *demand;       // [n+1]
@@ -109,7 +111,7 @@ struct AntBuffers {
   int *feasible;           // [m]
   int *steps;              // [m]
   uint32_t *draws;         // [m]
-  long long *loads;        // [m][K]  per-vehicle load (repair scratch)
+  int *loads;              // [m][K]  per-vehicle load (repair scratch)
   int *rep;                // [m][n]  repair additions (scratch)
   int *repc;               // [m][K]  repair additions per vehicle (scratch)
 };

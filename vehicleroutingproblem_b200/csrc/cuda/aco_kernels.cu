@@ -187,25 +187,21 @@ cudaError_t launch_weights(const InstanceView &iv, const PheromoneView &pv,
 // Construction
 // ===========================================================================
 
-// Per-lane Philox block of the current 128-draw batch.  Draw d of an ant is
-// word d%4 of Philox({d/4, ant, epoch, stream}, {seed, kDrawKey1}) >> 8; lane
-// L of batch b holds block 32 b + L.
-struct DrawBuf {
+// Draws of one ant, 128 at a time in a per-warp shared buffer: draw d is
+// word d%4 of Philox({d/4, ant, epoch, stream}, {seed, kDrawKey1}) >> 8;
+// lane L computes block 32 b + L of batch b and stores its 4 words.
+__device__ __forceinline__ void draw_refill(uint32_t *buf, uint32_t d,
+                                            uint32_t seed, uint32_t epoch,
+                                            uint32_t ant, uint32_t stream,
+                                            int lane) {
   uint32_t r[4];
-  uint32_t d;
-};
-
-__device__ __forceinline__ void draw_fill(DrawBuf &db, uint32_t seed,
-                                          uint32_t epoch, uint32_t ant,
-                                          uint32_t stream, int lane) {
-  uint32_t blk = ((db.d >> 7) << 5) + (uint32_t)lane;
-  philox4x32_10(blk, ant, epoch, stream, seed, kDrawKey1, db.r);
-}
-
-__device__ __forceinline__ uint32_t draw_peek(const DrawBuf &db) {
-  uint32_t w = db.d & 3u;
-  uint32_t v = (w == 0) ? db.r[0] : (w == 1) ? db.r[1] : (w == 2) ? db.r[2] : db.r[3];
-  return __shfl_sync(kFull, v, (db.d >> 2) & 31u) >> (32 - kDrawBits);
+  philox4x32_10(((d >> 7) << 5) + (uint32_t)lane, ant, epoch, stream, seed,
+                kDrawKey1, r);
+  __syncwarp();
+  uint4 v = make_uint4(r[0] >> (32 - kDrawBits), r[1] >> (32 - kDrawBits),
+                       r[2] >> (32 - kDrawBits), r[3] >> (32 - kDrawBits));
+  reinterpret_cast<uint4 *>(buf)[lane] = v;
+  __syncwarp();
 }
 
 template <int L, bool UNIT>
@@ -217,7 +213,7 @@ struct Tables {
   const float2 *coords;
   const int *dem;
 
-  __device__ __forceinline__ uint32_t weight(size_t idx) const {
+  __device__ __forceinline__ uint32_t weight(int idx) const {
     if (L == kLayoutSmemPacked) return lut[rel[idx]];
     return w[idx];
   }
@@ -225,38 +221,92 @@ struct Tables {
     if (L == kLayoutGlobal) return __ldg(coords + node);
     return coords[node];
   }
-  __device__ __forceinline__ long long demand(int node) const {
+  __device__ __forceinline__ int demand(int node) const {
     if (UNIT) return 1;
-    if (L == kLayoutGlobal) return (long long)__ldg(dem + node);
-    return (long long)dem[node];
+    if (L == kLayoutGlobal) return __ldg(dem + node);
+    return dem[node];
+  }
+};
+
+// Visited set of one ant.  V = 1 or 2: lane L holds bitmap words L (and
+// L + 32) in registers (n < 2048); V = 0: the bitmap is in shared memory.
+// The depot and the bits past node n start set.  test/set are collective.
+__device__ __forceinline__ uint32_t vis_init_word(int wi, int n) {
+  uint32_t word = 0u;
+  const int lo = wi << 5;
+  if (lo == 0) word |= 1u;
+  const int valid = n + 1 - lo;  // nodes lo..n in this word
+  if (valid < 32) word |= (valid <= 0) ? 0xffffffffu : (0xffffffffu << valid);
+  return word;
+}
+
+template <int V>
+struct Visited {
+  uint32_t w0, w1;
+  uint32_t *s;
+  int vw;
+
+  __device__ __forceinline__ void init(uint32_t *smem_words, int vw_, int n,
+                                       int lane) {
+    vw = vw_;
+    s = smem_words;
+    w0 = w1 = 0xffffffffu;
+    if (V >= 1) w0 = vis_init_word(lane, n);
+    if (V == 2) w1 = vis_init_word(lane + 32, n);
+    if (V == 0) {
+      for (int wi = lane; wi < vw; wi += 32) s[wi] = vis_init_word(wi, n);
+      __syncwarp();
+    }
+  }
+  __device__ __forceinline__ bool test(int c) const {
+    if (V == 0) return (s[c >> 5] >> (c & 31)) & 1u;
+    const int src = (c >> 5) & 31;
+    uint32_t word = __shfl_sync(kFull, w0, src);
+    if (V == 2) {
+      const uint32_t hi = __shfl_sync(kFull, w1, src);
+      word = (c >> 10) ? hi : word;
+    }
+    return (word >> (c & 31)) & 1u;
+  }
+  __device__ __forceinline__ void set(int node, int lane) {
+    const uint32_t bit = 1u << (node & 31);
+    if (V == 0) {
+      if (lane == 0) s[node >> 5] |= bit;
+      __syncwarp();
+    } else if (lane == ((node >> 5) & 31)) {
+      if (V == 2 && (node >> 10)) w1 |= bit; else w0 |= bit;
+    }
   }
 };
 
 // Nearest unvisited customer that fits (find_nearest_unvisited,
 // src/seq/aco_sequential.c:477-493: strict '<' over ascending nodes, so the
 // lowest index wins ties).  0 if none.
-template <int L, bool UNIT>
+template <int L, bool UNIT, int V>
 __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
-                                                 const uint32_t *vis, int vw,
-                                                 float2 pc, long long load,
-                                                 long long cap, int lane) {
+                                                 const Visited<V> &vis,
+                                                 float2 pc, int room,
+                                                 bool check_dem, int lane) {
   uint32_t best_h = 0xffffffffu, best_n = 0xffffffffu;
-  for (int wi = lane; wi < vw; wi += 32) {
-    uint32_t fr = ~vis[wi];
+  auto scan = [&](uint32_t fr, int wi) {
     while (fr) {
-      int b = __ffs(fr) - 1;
+      const int b = __ffs(fr) - 1;
       fr &= fr - 1;
-      int node = (wi << 5) + b;
-      if (!UNIT && load + tb.demand(node) > cap) continue;
-      uint32_t h = __float_as_uint(dist2f(pc, tb.coord(node)));
+      const int node = (wi << 5) + b;
+      if (!UNIT && check_dem && tb.demand(node) > room) continue;
+      const uint32_t h = __float_as_uint(dist2f(pc, tb.coord(node)));
       if (h < best_h) {
         best_h = h;
         best_n = (uint32_t)node;
       }
     }
-  }
-  uint32_t mh = __reduce_min_sync(kFull, best_h);
-  uint32_t mn = __reduce_min_sync(kFull, best_h == mh ? best_n : 0xffffffffu);
+  };
+  if (V >= 1) scan(~vis.w0, lane);
+  if (V == 2) scan(~vis.w1, lane + 32);
+  if (V == 0)
+    for (int wi = lane; wi < vis.vw; wi += 32) scan(~vis.s[wi], wi);
+  const uint32_t mh = __reduce_min_sync(kFull, best_h);
+  const uint32_t mn = __reduce_min_sync(kFull, best_h == mh ? best_n : 0xffffffffu);
   return (mh == 0xffffffffu) ? 0 : (int)mn;
 }
 
@@ -272,88 +322,105 @@ struct ConstructArgs {
   int use_state_epoch;  // 1: epoch number = st->epoch (graph replays)
 };
 
+// FP64 cost of a compact route sequence, summed in route order
+// (solution_cost, src/common/solution.c:126-137).  Lanes compute the arc
+// lengths, the sum runs in order in every lane; the (0,0) pairs between
+// consecutive routes add +0.0, which leaves the sum unchanged.
+template <int L, bool UNIT>
+__device__ __forceinline__ double route_cost(const Tables<L, UNIT> &tb,
+                                             const int *route, int entries,
+                                             int lane) {
+  double acc = 0.0;
+  const int arcs = entries - 1;
+  for (int b = 0; b < arcs; b += 32) {
+    const int j = b + lane;
+    double dj = 0.0;
+    if (j < arcs) dj = dist64(tb.coord(route[j]), tb.coord(route[j + 1]));
+    const int cnt = (arcs - b < 32) ? arcs - b : 32;
+    for (int t = 0; t < cnt; ++t) acc = __dadd_rn(acc, __shfl_sync(kFull, dj, t));
+  }
+  return acc;
+}
+
 // One ant, one warp.  Rules of build_ant_solution
 // (src/seq/aco_sequential.c:616-681) with the demand extension:
 //   vehicle v extends while remaining > 0, remaining demand > (K-v-1) Q and
 //   load < Q; the next customer is drawn by roulette over the eligible
 //   candidates (unvisited, load + d <= Q), else the nearest eligible one;
 //   customers left over are added by the backward repair pass.
-template <int L, bool UNIT>
+template <int L, bool UNIT, int V>
 __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
-                          uint32_t *vis, int ant, uint32_t epoch, int lane) {
+                          Visited<V> &vis, uint32_t *dbuf, int ant,
+                          uint32_t epoch, int lane) {
   const InstanceView &iv = a.iv;
-  const int k = iv.k, K = iv.K, R = iv.route_stride, vw = a.plan.vis_words;
-  const long long cap = iv.cap;
+  const int k = iv.k, K = iv.K, R = iv.route_stride;
+  const int cap = (int)iv.cap;
+  const int max_dem = iv.max_demand;
   int *route = a.ab.routes + (size_t)ant * R;
   int *lens = a.ab.lens + (size_t)ant * K;
-  long long *loads = a.ab.loads + (size_t)ant * K;
+  int *loads = a.ab.loads + (size_t)ant * K;
 
-  DrawBuf db;
-  db.d = 0;
-  draw_fill(db, a.seed, epoch, (uint32_t)ant, a.stream, lane);
-  uint32_t r_next = draw_peek(db);
+  uint32_t d = 0;
+  draw_refill(dbuf, d, a.seed, epoch, (uint32_t)ant, a.stream, lane);
+  uint32_t r_next = dbuf[0];
 
-  long long remaining = iv.n;
-  long long rem_dem = iv.total_demand;
-  double cost = 0.0;
+  int remaining = iv.n;
+  int rem_dem = (int)iv.total_demand;
   int pos = 0;
-  const float2 depot = tb.coord(0);
 
   for (int v = 0; v < K; ++v) {
     const int start = pos;
     if (lane == 0) route[pos] = 0;
     ++pos;
     int cur = 0;
-    float2 pc = depot;
-    long long load = 0;
-    const long long future = (long long)(K - v - 1) * cap;
-    while (remaining > 0 && rem_dem > future && load < cap) {
-      const size_t base = (size_t)cur * k;
-      int c = 0;
+    int load = 0;
+    const long long fut64 = (long long)(K - v - 1) * iv.cap;
+    const int future = fut64 > 0x7fffffffLL ? 0x7fffffff : (int)fut64;
+    int room = cap;
+    bool tight = !UNIT && room < max_dem;
+    // Every demand is >= 1, so rem_dem > future >= 0 implies remaining > 0.
+    while (rem_dem > future && load < cap) {
+      const int base = cur * k;
+      int c = 0, dc = 1;
       uint32_t w = 0u;
       if (lane < k) {
         c = tb.cand[base + lane];
         w = tb.weight(base + lane);
       }
-      bool ok = ((vis[c >> 5] >> (c & 31)) & 1u) == 0u;
-      if (!UNIT) ok = ok && (load + tb.demand(c) <= cap);
+      if (!UNIT) dc = tb.demand(c);
+      bool ok = !vis.test(c);
+      if (!UNIT) ok = ok && (!tight || dc <= room);
       const uint32_t wv = ok ? w : 0u;
+      const uint32_t denom = __reduce_add_sync(kFull, wv);
       const uint32_t cum = warp_incl_scan(wv, lane);
-      const uint32_t denom = __shfl_sync(kFull, cum, 31);
-      int next;
-      if (denom != 0u) {
-        const unsigned long long T = (unsigned long long)r_next * denom;
-        const bool sel = (wv != 0u) && (((unsigned long long)cum << kDrawBits) >= T);
-        const unsigned m = __ballot_sync(kFull, sel);
-        // m is never empty: at the last eligible lane cum = denom and
-        // r < 2^24.  The guard keeps the shuffle source in range regardless.
-        next = m ? __shfl_sync(kFull, c, __ffs(m) - 1) : 0;
-        ++db.d;
-        if ((db.d & 127u) == 0u) draw_fill(db, a.seed, epoch, (uint32_t)ant, a.stream, lane);
-        r_next = draw_peek(db);
+      // cum * 2^24 >= r * denom  <=>  cum >= ceil(r * denom / 2^24)
+      const uint32_t thr =
+          (uint32_t)(((unsigned long long)r_next * denom + 0xFFFFFFull) >> kDrawBits);
+      const unsigned m = __ballot_sync(kFull, wv != 0u && cum >= thr);
+      const int src = m ? __ffs(m) - 1 : 0;
+      int next = __shfl_sync(kFull, c, src);
+      int dn = UNIT ? 1 : __shfl_sync(kFull, dc, src);
+      if (denom == 0u) {
+        next = nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), room, tight, lane);
         if (next <= 0) break;
+        dn = tb.demand(next);
       } else {
-        next = nearest_unvisited<L, UNIT>(tb, vis, vw, pc, load, cap, lane);
-        if (next <= 0) break;
+        ++d;
+        if ((d & 127u) == 0u) draw_refill(dbuf, d, a.seed, epoch, (uint32_t)ant, a.stream, lane);
+        r_next = dbuf[d & 127u];
       }
-      const float2 pn = tb.coord(next);
-      if (lane == 0) {
-        route[pos] = next;
-        vis[next >> 5] |= 1u << (next & 31);
-        cost = __dadd_rn(cost, dist64(pc, pn));
-      }
-      __syncwarp();
+      if (lane == 0) route[pos] = next;
+      vis.set(next, lane);
       ++pos;
-      const long long dn = tb.demand(next);
-      load += dn;
       --remaining;
+      load += dn;
       rem_dem -= dn;
+      room = cap - load;
+      tight = !UNIT && room < max_dem;
       cur = next;
-      pc = pn;
     }
     if (lane == 0) {
       route[pos] = 0;
-      cost = __dadd_rn(cost, dist64(pc, depot));
       lens[v] = pos + 1 - start;
       loads[v] = load;
     }
@@ -374,22 +441,18 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       const int len_v = lens[v];
       off_end -= len_v;
       int cur = route[off_end + len_v - 2];
-      float2 pc = tb.coord(cur);
-      long long load = loads[v];
+      int load = loads[v];
       int cnt = 0;
       while (remaining > 0 && load < cap) {
-        int next = nearest_unvisited<L, UNIT>(tb, vis, vw, pc, load, cap, lane);
+        const int next = nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), cap - load,
+                                                       true, lane);
         if (next <= 0) break;
-        if (lane == 0) {
-          rep[nrep + cnt] = next;
-          vis[next >> 5] |= 1u << (next & 31);
-        }
-        __syncwarp();
+        if (lane == 0) rep[nrep + cnt] = next;
+        vis.set(next, lane);
         ++cnt;
         load += tb.demand(next);
         --remaining;
         cur = next;
-        pc = tb.coord(next);
       }
       if (lane == 0) repc[v] = cnt;
       nrep += cnt;
@@ -414,29 +477,21 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
         lens[v] = len_v + cnt;
         add_after += cnt;
       }
-      pos += nrep;
-      // FP64 cost in final route order (solution_cost, solution.c:126-137).
-      cost = 0.0;
-      int off = 0;
-      for (int v = 0; v < K; ++v) {
-        for (int t = 1; t < lens[v]; ++t)
-          cost = __dadd_rn(cost, dist64(tb.coord(route[off + t - 1]), tb.coord(route[off + t])));
-        off += lens[v];
-      }
     }
-    __syncwarp();
+    pos += nrep;
   }
-
+  __syncwarp();
+  const double cost = route_cost<L, UNIT>(tb, route, pos, lane);
   if (lane == 0) {
     a.ab.cost[ant] = cost;
     a.ab.feasible[ant] = (remaining == 0) ? 1 : 0;
     a.ab.steps[ant] = pos - K;
-    a.ab.draws[ant] = db.d;
+    a.ab.draws[ant] = d;
   }
 }
 
-template <int L, bool UNIT>
-__global__ void __launch_bounds__(1024, 1) k_construct(ConstructArgs a) {
+template <int L, bool UNIT, int V>
+__global__ void __launch_bounds__(512, 1) k_construct(ConstructArgs a) {
   if (a.st && *(volatile int *)&a.st->skip) return;
   extern __shared__ __align__(128) unsigned char smem[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -465,14 +520,14 @@ __global__ void __launch_bounds__(1024, 1) k_construct(ConstructArgs a) {
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      uint32_t total = pl.bytes_cand + pl.bytes_w + pl.bytes_coords + (UNIT ? 0u : pl.bytes_dem);
+      const uint32_t total = pl.bytes_cand + pl.bytes_w + pl.bytes_coords + (UNIT ? 0u : pl.bytes_dem);
       mbar_arrive_expect_tx(bar, total);
       const uint32_t kChunk = 32768u;
       auto issue = [&](unsigned char *dst, const void *src, uint32_t bytes) {
-        const unsigned char *s = reinterpret_cast<const unsigned char *>(src);
+        const unsigned char *sp = reinterpret_cast<const unsigned char *>(src);
         for (uint32_t o = 0; o < bytes; o += kChunk) {
-          uint32_t b = bytes - o < kChunk ? bytes - o : kChunk;
-          bulk_g2s(dst + o, s + o, b, bar);
+          const uint32_t b = bytes - o < kChunk ? bytes - o : kChunk;
+          bulk_g2s(dst + o, sp + o, b, bar);
         }
       };
       issue(smem + pl.off_cand, iv.cand, pl.bytes_cand);
@@ -484,22 +539,14 @@ __global__ void __launch_bounds__(1024, 1) k_construct(ConstructArgs a) {
     if (L == kLayoutSmemPacked) {
       uint32_t *lut = reinterpret_cast<uint32_t *>(smem + pl.off_lut);
       for (int r = threadIdx.x; r < 256; r += blockDim.x) lut[r] = __ldg(a.et.lut + r);
+      __syncthreads();
     }
   }
 
-  // Visited bitmap of this warp's ant: the depot and the bits past node n
-  // are set so that scans see customers only.
-  uint32_t *vis = reinterpret_cast<uint32_t *>(smem + pl.off_vis) + (size_t)warp * pl.vis_words;
-  for (int wi = lane; wi < pl.vis_words; wi += 32) {
-    uint32_t word = 0u;
-    int lo = wi << 5;
-    if (lo == 0) word |= 1u;
-    int valid = iv.n + 1 - lo;  // nodes lo..n in this word
-    if (valid < 32) word |= (valid <= 0) ? 0xffffffffu : (0xffffffffu << valid);
-    vis[wi] = word;
-  }
-  if (L == kLayoutSmemPacked) __syncthreads();
-  __syncwarp();
+  uint32_t *dbuf = reinterpret_cast<uint32_t *>(smem + pl.off_draw) + (size_t)warp * 128;
+  Visited<V> vis;
+  vis.init(reinterpret_cast<uint32_t *>(smem + pl.off_vis) + (size_t)warp * pl.vis_words,
+           pl.vis_words, iv.n, lane);
 
   if (L != kLayoutGlobal) {
     if (!mbar_wait_bounded(bar, 0, 1u << 22)) {
@@ -511,7 +558,7 @@ __global__ void __launch_bounds__(1024, 1) k_construct(ConstructArgs a) {
   const int ant = blockIdx.x * pl.wpb + warp;
   if (ant >= iv.m) return;
   const uint32_t epoch = a.use_state_epoch ? (uint32_t)a.st->epoch : a.epoch;
-  build_ant<L, UNIT>(a, tb, vis, ant, epoch, lane);
+  build_ant<L, UNIT, V>(a, tb, vis, dbuf, ant, epoch, lane);
 }
 
 static int g_max_smem = 0;
@@ -533,14 +580,16 @@ SmemPlan plan_construct(const InstanceView &iv, int layout, int num_sms,
   SmemPlan p = {};
   const size_t rows = (size_t)iv.n + 1;
   p.vis_words = (int)((rows + 31) / 32);
+  p.vreg = p.vis_words <= 32 ? 1 : (p.vis_words <= 64 ? 2 : 0);
   int wpb = (iv.m + num_sms - 1) / num_sms;
   if (wpb < 1) wpb = 1;
-  if (wpb > 32) wpb = 32;
+  if (wpb > 16) wpb = 16;
   p.wpb = wpb;
   p.bytes_cand = pad16(rows * iv.k * sizeof(uint16_t));
   p.bytes_coords = pad16(rows * sizeof(float2));
   p.bytes_dem = iv.unit ? 0u : pad16(rows * sizeof(int));
-  const uint32_t vis_bytes = (uint32_t)wpb * p.vis_words * 4u;
+  const uint32_t vis_bytes = p.vreg ? 0u : (uint32_t)wpb * p.vis_words * 4u;
+  const uint32_t draw_bytes = (uint32_t)wpb * 512u;
   auto finish = [&](int lay) {
     p.layout = lay;
     uint32_t off = 16;  // mbarrier
@@ -555,6 +604,8 @@ SmemPlan plan_construct(const InstanceView &iv, int layout, int num_sms,
       p.off_dem = off; off += p.bytes_dem;
       p.off_lut = off; off += (lay == kLayoutSmemPacked) ? 1024u : 0u;
     }
+    p.off_draw = off;
+    off += draw_bytes;
     p.off_vis = off;
     off += vis_bytes;
     p.total = off;
@@ -571,29 +622,42 @@ SmemPlan plan_construct(const InstanceView &iv, int layout, int num_sms,
   return p;
 }
 
-template <int L, bool UNIT>
+template <int L, bool UNIT, int V>
 static cudaError_t configure_t() {
-  return cudaFuncSetAttribute(k_construct<L, UNIT>,
+  return cudaFuncSetAttribute(k_construct<L, UNIT, V>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               construct_max_smem());
+}
+
+template <int L, bool UNIT>
+static cudaError_t configure_lu() {
+  cudaError_t e = configure_t<L, UNIT, 0>();
+  if (e == cudaSuccess) e = configure_t<L, UNIT, 1>();
+  if (e == cudaSuccess) e = configure_t<L, UNIT, 2>();
+  return e;
 }
 
 // Opts every construct instantiation into the full shared-memory carve-out;
 // called once per device before any launch or graph capture.
 cudaError_t prepare_construct_kernels() {
-  cudaError_t e = configure_t<kLayoutSmemWeights, false>();
-  if (e == cudaSuccess) e = configure_t<kLayoutSmemWeights, true>();
-  if (e == cudaSuccess) e = configure_t<kLayoutSmemPacked, false>();
-  if (e == cudaSuccess) e = configure_t<kLayoutSmemPacked, true>();
-  if (e == cudaSuccess) e = configure_t<kLayoutGlobal, false>();
-  if (e == cudaSuccess) e = configure_t<kLayoutGlobal, true>();
+  cudaError_t e = configure_lu<kLayoutSmemWeights, false>();
+  if (e == cudaSuccess) e = configure_lu<kLayoutSmemWeights, true>();
+  if (e == cudaSuccess) e = configure_lu<kLayoutSmemPacked, false>();
+  if (e == cudaSuccess) e = configure_lu<kLayoutSmemPacked, true>();
+  if (e == cudaSuccess) e = configure_lu<kLayoutGlobal, false>();
+  if (e == cudaSuccess) e = configure_lu<kLayoutGlobal, true>();
   return e;
 }
 
 template <int L, bool UNIT>
-static cudaError_t launch_construct_t(const ConstructArgs &a, cudaStream_t s) {
+static cudaError_t launch_construct_lu(const ConstructArgs &a, cudaStream_t s) {
   const int grid = (a.iv.m + a.plan.wpb - 1) / a.plan.wpb;
-  k_construct<L, UNIT><<<grid, a.plan.wpb * 32, a.plan.total, s>>>(a);
+  const int threads = a.plan.wpb * 32;
+  switch (a.plan.vreg) {
+    case 1: k_construct<L, UNIT, 1><<<grid, threads, a.plan.total, s>>>(a); break;
+    case 2: k_construct<L, UNIT, 2><<<grid, threads, a.plan.total, s>>>(a); break;
+    default: k_construct<L, UNIT, 0><<<grid, threads, a.plan.total, s>>>(a); break;
+  }
   return cudaGetLastError();
 }
 
@@ -614,12 +678,12 @@ cudaError_t launch_construct(const InstanceView &iv, const EpochTables &et,
   a.use_state_epoch = use_state_epoch;
   if ((int)plan.total > construct_max_smem()) return cudaErrorInvalidValue;
   switch (plan.layout * 2 + (iv.unit ? 1 : 0)) {
-    case 0: return launch_construct_t<kLayoutSmemWeights, false>(a, s);
-    case 1: return launch_construct_t<kLayoutSmemWeights, true>(a, s);
-    case 2: return launch_construct_t<kLayoutSmemPacked, false>(a, s);
-    case 3: return launch_construct_t<kLayoutSmemPacked, true>(a, s);
-    case 4: return launch_construct_t<kLayoutGlobal, false>(a, s);
-    case 5: return launch_construct_t<kLayoutGlobal, true>(a, s);
+    case 0: return launch_construct_lu<kLayoutSmemWeights, false>(a, s);
+    case 1: return launch_construct_lu<kLayoutSmemWeights, true>(a, s);
+    case 2: return launch_construct_lu<kLayoutSmemPacked, false>(a, s);
+    case 3: return launch_construct_lu<kLayoutSmemPacked, true>(a, s);
+    case 4: return launch_construct_lu<kLayoutGlobal, false>(a, s);
+    case 5: return launch_construct_lu<kLayoutGlobal, true>(a, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -806,33 +870,107 @@ __device__ __forceinline__ void deposit_arc(const PheromoneView &pv,
 }
 
 // Deposit of one solution by one block.  Arcs of different routes touch
-// different cells, except the depot loop (0,0) of empty routes, so the arcs
-// of routes of >= 4 nodes are dealt round-robin over the threads; a
-// one-customer route [0 a 0] (whose two arcs share the cells {0,a}) is
-// walked by one thread, and all empty routes by thread 0 in vehicle order.
+// different cells, except the depot loop (0,0) of empty routes; inside a
+// route of >= 4 nodes all 2(len-1) cells are distinct too.  So: route
+// offsets are scanned into shared memory; the arcs of routes of >= 4 nodes
+// are dealt over all threads, each thread loading all its cells before it
+// stores any; a one-customer route [0 a 0] (whose two arcs share the cells
+// {0,a}) is walked by one thread in order, and all empty routes by thread 0
+// in vehicle order.  s_off holds K+1 ints, or is null for very large K
+// (then every thread walks the length list).
 __device__ void deposit_solution(const PheromoneView &pv, size_t stride,
                                  const int *nodes, const int *lens, int K,
-                                 float dep) {
+                                 float dep, int *s_off) {
   const int bd = (int)blockDim.x, tid = (int)threadIdx.x;
-  int off = 0, base = 0;  // node offset and arc count before route v
-  for (int v = 0; v < K; ++v) {
-    const int len = lens[v];
-    const int owner = base % bd;
-    if (len >= 4) {
-      for (int t = (tid - owner + bd) % bd; t < len - 1; t += bd)
-        deposit_arc(pv, stride, nodes[off + t], nodes[off + t + 1], dep);
-    } else if (len == 3) {
-      if (tid == owner) {
+  const int lane = tid & 31, warp = tid >> 5;
+  if (!s_off) {
+    int off = 0, base = 0;
+    for (int v = 0; v < K; ++v) {
+      const int len = lens[v];
+      const int owner = base % bd;
+      if (len >= 4) {
+        for (int t = (tid - owner + bd) % bd; t < len - 1; t += bd)
+          deposit_arc(pv, stride, nodes[off + t], nodes[off + t + 1], dep);
+      } else if (len == 3 && tid == owner) {
         deposit_arc(pv, stride, nodes[off], nodes[off + 1], dep);
         deposit_arc(pv, stride, nodes[off + 1], nodes[off + 2], dep);
+      } else if (len == 2 && tid == 0) {
+        deposit_arc(pv, stride, nodes[off], nodes[off + 1], dep);
       }
-    } else if (len == 2) {
-      if (tid == 0) deposit_arc(pv, stride, nodes[off], nodes[off + 1], dep);
+      off += len;
+      base += len > 1 ? len - 1 : 0;
     }
-    off += len;
-    base += len > 1 ? len - 1 : 0;
+    return;
+  }
+  if (warp == 0) {
+    int carry = 0;
+    for (int b = 0; b < K; b += 32) {
+      const int v = b + lane;
+      const int len = v < K ? lens[v] : 0;
+      const int inc = (int)warp_incl_scan((uint32_t)len, lane);
+      if (v < K) s_off[v + 1] = carry + inc;
+      carry += __shfl_sync(kFull, inc, 31);
+    }
+    if (lane == 0) s_off[0] = 0;
+  }
+  __syncthreads();
+  const int total = s_off[K];
+  constexpr int kBatch = 4;
+  for (int j0 = tid; j0 < total; j0 += kBatch * bd) {
+    int us[kBatch], cs[kBatch];
+    bool valid[kBatch];
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      const int j = j0 + q * bd;
+      valid[q] = false;
+      us[q] = cs[q] = 0;
+      if (j < total) {
+        int lo = 0, hi = K;  // route v with s_off[v] <= j < s_off[v+1]
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (s_off[mid] <= j) lo = mid; else hi = mid;
+        }
+        const int off = s_off[lo], len = s_off[lo + 1] - off;
+        if (len >= 4 && j > off) {
+          valid[q] = true;
+          us[q] = nodes[j - 1];
+          cs[q] = nodes[j];
+        }
+      }
+    }
+    uint8_t fq[kBatch], rq[kBatch];
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      fq[q] = rq[q] = 0;
+      if (valid[q]) {
+        fq[q] = ld_cg_u8(pv.tau + (size_t)us[q] * stride + cs[q]);
+        rq[q] = ld_cg_u8(pv.tau + (size_t)cs[q] * stride + us[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      if (valid[q]) {
+        const uint8_t nq = quant(dequant(fq[q], pv.log_min, pv.log_step) + dep, pv.log_min,
+                                 pv.log_step, pv.q_min, pv.q_max);
+        if (nq > fq[q]) st_cg_u8(pv.tau + (size_t)us[q] * stride + cs[q], nq);
+        if (nq > rq[q]) st_cg_u8(pv.tau + (size_t)cs[q] * stride + us[q], nq);
+      }
+    }
+  }
+  for (int v = tid; v < K; v += bd) {
+    const int off = s_off[v];
+    if (s_off[v + 1] - off == 3) {
+      deposit_arc(pv, stride, nodes[off], nodes[off + 1], dep);
+      deposit_arc(pv, stride, nodes[off + 1], nodes[off + 2], dep);
+    }
+  }
+  if (tid == 0) {
+    for (int v = 0; v < K; ++v)
+      if (s_off[v + 1] - s_off[v] == 2) deposit_arc(pv, stride, 0, 0, dep);
   }
 }
+
+constexpr int kDepositSmemRoutes = 4096;
 
 __device__ __forceinline__ uint32_t evap4(uint32_t x, uint32_t floor4,
                                           uint32_t delta4) {
@@ -899,11 +1037,13 @@ __global__ void __launch_bounds__(512) k_evap_deposit(EvapArgs a) {
   const int best = a.st ? a.st->best_ant : a.best_ant;
   const float dep_i = a.st ? a.st->dep_iter : a.dep_iter;
   const float dep_g = a.st ? a.st->dep_global : a.dep_global;
+  extern __shared__ int s_off[];
+  int *offs = (a.iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
   deposit_solution(pv, stride_n, a.ab.routes + (size_t)best * a.iv.route_stride,
-                   a.ab.lens + (size_t)best * a.iv.K, a.iv.K, dep_i);
+                   a.ab.lens + (size_t)best * a.iv.K, a.iv.K, dep_i, offs);
   __syncthreads();
   if (a.gbest_nodes) {
-    deposit_solution(pv, stride_n, a.gbest_nodes, a.gbest_lens, a.iv.K, dep_g);
+    deposit_solution(pv, stride_n, a.gbest_nodes, a.gbest_lens, a.iv.K, dep_g, offs);
   }
   if (threadIdx.x == 0) *a.counter = 0u;
 }
@@ -923,7 +1063,8 @@ cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
   a.counter = counter;
   a.best_ant = 0;
   a.dep_iter = a.dep_global = 0.0f;
-  k_evap_deposit<<<grid, 512, 0, s>>>(a);
+  const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
+  k_evap_deposit<<<grid, 512, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -948,7 +1089,8 @@ cudaError_t launch_evap_deposit_explicit(const InstanceView &iv,
   a.best_ant = best_ant;
   a.dep_iter = dep_iter;
   a.dep_global = dep_global;
-  k_evap_deposit<<<grid, 512, 0, s>>>(a);
+  const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
+  k_evap_deposit<<<grid, 512, smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -290,6 +290,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   }
   const int n = p->n;
   long long total_demand = n;
+  int max_demand = 1;
   bool unit = true;
   if (p->demand) {
     if (p->demand[0] != 0) return ACO_ERR_INVALID_INPUT;
@@ -297,8 +298,14 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
     for (int j = 1; j <= n; ++j) {
       if (p->demand[j] < 1) return ACO_ERR_INVALID_INPUT;
       if (p->demand[j] != 1) unit = false;
+      if (p->demand[j] > max_demand) max_demand = p->demand[j];
       total_demand += p->demand[j];
     }
+  }
+  // Loads and remaining demand are 32-bit on the device.
+  if (total_demand > 0x7fffffffLL || p->capacity > 0x7fffffffLL) {
+    fprintf(stderr, "aco_b200: total demand and capacity must be below 2^31\n");
+    return ACO_ERR_INVALID_INPUT;
   }
   int k = p->cand_k > 0 ? p->cand_k : 32;
   if (k > kMaxCand) k = kMaxCand;
@@ -370,6 +377,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   iv.cap = p->capacity;
   iv.total_demand = total_demand;
   iv.unit = unit ? 1 : 0;
+  iv.max_demand = max_demand;
   iv.route_stride = R;
   iv.coords = ctx->d_coords;
   iv.demand = ctx->d_demand;

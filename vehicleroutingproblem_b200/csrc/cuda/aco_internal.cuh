@@ -282,5 +282,203 @@ __device__ __forceinline__ void st_cg_u8(uint8_t *p, uint8_t v) {
   asm volatile("st.global.cg.u8 [%0], %1;" ::"l"(p), "h"(w) : "memory");
 }
 
+// Warp-wide k-nearest selection for node i: the k smallest keys
+// (d^2 bits << 32 | j) over j in 1..n, j != i.  Lane t < k ends holding the
+// t-th smallest (~0 when fewer than k exist).  Keys are unique, so the order
+// is total: ascending d^2, ties to the lower j, as the reference's insertion
+// with a strict '<' (aco_cuda_kernels.cu:187-201).
+__device__ inline unsigned long long warp_knn(const float2 *coords, int n, int k,
+                                       int i, int lane) {
+  const unsigned long long kNone = ~0ull;
+  unsigned long long list = kNone;
+  unsigned long long kth = kNone;
+  const float2 pi = coords[i];
+  for (int base = 1; base <= n; base += 32) {
+    int j = base + lane;
+    unsigned long long key = kNone;
+    if (j <= n && j != i) {
+      float d2 = dist2f(pi, __ldg(coords + j));
+      key = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)j;
+    }
+    unsigned m = __ballot_sync(kFull, key < kth);
+    while (m) {
+      int b = __ffs(m) - 1;
+      m &= m - 1;
+      unsigned long long x = __shfl_sync(kFull, key, b);
+      if (x < kth) {
+        int pos = __popc(__ballot_sync(kFull, lane < k && list < x));
+        unsigned long long up = __shfl_up_sync(kFull, list, 1);
+        if (lane > pos) list = up;
+        else if (lane == pos) list = x;
+        kth = __shfl_sync(kFull, list, k - 1);
+      }
+    }
+  }
+  return list;
+}
+
+// ---------------------------------------------------------------------------
+// Pheromone deposit (shared by the native kernels and the drop-in kernels)
+// ---------------------------------------------------------------------------
+// Route layouts a deposit can read: node t of route v, whose first node is
+// entry off_v of the compact sequence (K segments [0 .. 0] back to back).
+struct CompactNodes {  // compact sequence (this library's layout)
+  const int *p;
+  __device__ __forceinline__ int operator()(int v, int off_v, int t) const {
+    return p[off_v + t];
+  }
+};
+struct InterleavedNodes {  // reference: routes[step * m + ant], shared depots
+  const int *p;
+  int m, ant;
+  __device__ __forceinline__ int operator()(int v, int off_v, int t) const {
+    return p[(size_t)(off_v - v + t) * m + ant];
+  }
+};
+struct FlatNodes {  // reference global-best buffer: flat[v * (n+1) + t]
+  const int *p;
+  int stride;
+  __device__ __forceinline__ int operator()(int v, int off_v, int t) const {
+    return p[(size_t)v * stride + t];
+  }
+};
+
+// quantize_tau / dequantize_tau of the reference (aco_cuda_kernels.cu:25-45),
+// the same expressions so that the device math rounds identically.
+__device__ __forceinline__ float dequant(uint8_t q, float log_min, float log_step) {
+  return expf((float)q * log_step + log_min);
+}
+
+__device__ __forceinline__ uint8_t quant(float tau, float log_min,
+                                         float log_step, uint8_t q_min,
+                                         uint8_t q_max) {
+  if (tau <= 0.0f) return q_min;
+  float log_t = logf(tau);
+  float q_f = (log_t - log_min) / log_step;
+  if (q_f <= (float)q_min) return q_min;
+  if (q_f >= (float)q_max) return q_max;
+  return (uint8_t)roundf(q_f);
+}
+
+// One arc (u, c): new = quantize(dequantize(tau[u][c]) + dep), max-ed into
+// tau[u][c] and tau[c][u] (aco_cuda_kernels.cu:614-623).  The caller
+// guarantees that no other thread touches these two cells concurrently.
+__device__ __forceinline__ void deposit_arc(const PheromoneView &pv,
+                                            size_t stride, int u, int c,
+                                            float dep) {
+  uint8_t *fwd = pv.tau + (size_t)u * stride + c;
+  uint8_t *rev = pv.tau + (size_t)c * stride + u;
+  const uint8_t old = ld_cg_u8(fwd);
+  const uint8_t nq = quant(dequant(old, pv.log_min, pv.log_step) + dep,
+                           pv.log_min, pv.log_step, pv.q_min, pv.q_max);
+  if (nq > old) st_cg_u8(fwd, nq);
+  const uint8_t oldr = ld_cg_u8(rev);
+  if (nq > oldr) st_cg_u8(rev, nq);
+}
+
+// Deposit of one solution by one block.  Arcs of different routes touch
+// different cells, except the depot loop (0,0) of empty routes; inside a
+// route of >= 4 nodes all 2(len-1) cells are distinct too.  So: route
+// offsets are scanned into shared memory; the arcs of routes of >= 4 nodes
+// are dealt over all threads, each thread loading all its cells before it
+// stores any; a one-customer route [0 a 0] (whose two arcs share the cells
+// {0,a}) is walked by one thread in order, and all empty routes by thread 0
+// in vehicle order.  s_off holds K+1 ints, or is null for very large K
+// (then every thread walks the length list).
+template <class Nodes>
+__device__ void deposit_solution(const PheromoneView &pv, size_t stride,
+                                 const Nodes &nodes, const int *lens, int K,
+                                 float dep, int *s_off) {
+  const int bd = (int)blockDim.x, tid = (int)threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  if (!s_off) {
+    int off = 0, base = 0;
+    for (int v = 0; v < K; ++v) {
+      const int len = lens[v];
+      const int owner = base % bd;
+      if (len >= 4) {
+        for (int t = (tid - owner + bd) % bd; t < len - 1; t += bd)
+          deposit_arc(pv, stride, nodes(v, off, t), nodes(v, off, t + 1), dep);
+      } else if (len == 3 && tid == owner) {
+        deposit_arc(pv, stride, nodes(v, off, 0), nodes(v, off, 1), dep);
+        deposit_arc(pv, stride, nodes(v, off, 1), nodes(v, off, 2), dep);
+      } else if (len == 2 && tid == 0) {
+        deposit_arc(pv, stride, nodes(v, off, 0), nodes(v, off, 1), dep);
+      }
+      off += len;
+      base += len > 1 ? len - 1 : 0;
+    }
+    return;
+  }
+  if (warp == 0) {
+    int carry = 0;
+    for (int b = 0; b < K; b += 32) {
+      const int v = b + lane;
+      const int len = v < K ? lens[v] : 0;
+      const int inc = (int)warp_incl_scan((uint32_t)len, lane);
+      if (v < K) s_off[v + 1] = carry + inc;
+      carry += __shfl_sync(kFull, inc, 31);
+    }
+    if (lane == 0) s_off[0] = 0;
+  }
+  __syncthreads();
+  const int total = s_off[K];
+  constexpr int kBatch = 4;
+  for (int j0 = tid; j0 < total; j0 += kBatch * bd) {
+    int us[kBatch], cs[kBatch];
+    bool valid[kBatch];
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      const int j = j0 + q * bd;
+      valid[q] = false;
+      us[q] = cs[q] = 0;
+      if (j < total) {
+        int lo = 0, hi = K;  // route v with s_off[v] <= j < s_off[v+1]
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (s_off[mid] <= j) lo = mid; else hi = mid;
+        }
+        const int off = s_off[lo], len = s_off[lo + 1] - off;
+        if (len >= 4 && j > off) {
+          valid[q] = true;
+          us[q] = nodes(lo, off, j - off - 1);
+          cs[q] = nodes(lo, off, j - off);
+        }
+      }
+    }
+    uint8_t fq[kBatch], rq[kBatch];
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      fq[q] = rq[q] = 0;
+      if (valid[q]) {
+        fq[q] = ld_cg_u8(pv.tau + (size_t)us[q] * stride + cs[q]);
+        rq[q] = ld_cg_u8(pv.tau + (size_t)cs[q] * stride + us[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kBatch; ++q) {
+      if (valid[q]) {
+        const uint8_t nq = quant(dequant(fq[q], pv.log_min, pv.log_step) + dep, pv.log_min,
+                                 pv.log_step, pv.q_min, pv.q_max);
+        if (nq > fq[q]) st_cg_u8(pv.tau + (size_t)us[q] * stride + cs[q], nq);
+        if (nq > rq[q]) st_cg_u8(pv.tau + (size_t)cs[q] * stride + us[q], nq);
+      }
+    }
+  }
+  for (int v = tid; v < K; v += bd) {
+    const int off = s_off[v];
+    if (s_off[v + 1] - off == 3) {
+      deposit_arc(pv, stride, nodes(v, off, 0), nodes(v, off, 1), dep);
+      deposit_arc(pv, stride, nodes(v, off, 1), nodes(v, off, 2), dep);
+    }
+  }
+  if (tid == 0) {
+    for (int v = 0; v < K; ++v)
+      if (s_off[v + 1] - s_off[v] == 2) deposit_arc(pv, stride, 0, 0, dep);
+  }
+}
+
+constexpr int kDepositSmemRoutes = 4096;
+
 }  // namespace acob200
 #endif

@@ -35,41 +35,6 @@ __device__ __forceinline__ int level_of(float d2, const float *thr, int J) {
   return lo;
 }
 
-// Warp-wide k-nearest selection for node i: the k smallest keys
-// (d^2 bits << 32 | j) over j in 1..n, j != i.  Lane t < k ends holding the
-// t-th smallest (~0 when fewer than k exist).  Keys are unique, so the order
-// is total: ascending d^2, ties to the lower j, as the reference's insertion
-// with a strict '<' (aco_cuda_kernels.cu:187-201).
-__device__ unsigned long long warp_knn(const float2 *coords, int n, int k,
-                                       int i, int lane) {
-  const unsigned long long kNone = ~0ull;
-  unsigned long long list = kNone;
-  unsigned long long kth = kNone;
-  const float2 pi = coords[i];
-  for (int base = 1; base <= n; base += 32) {
-    int j = base + lane;
-    unsigned long long key = kNone;
-    if (j <= n && j != i) {
-      float d2 = dist2f(pi, __ldg(coords + j));
-      key = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)j;
-    }
-    unsigned m = __ballot_sync(kFull, key < kth);
-    while (m) {
-      int b = __ffs(m) - 1;
-      m &= m - 1;
-      unsigned long long x = __shfl_sync(kFull, key, b);
-      if (x < kth) {
-        int pos = __popc(__ballot_sync(kFull, lane < k && list < x));
-        unsigned long long up = __shfl_up_sync(kFull, list, 1);
-        if (lane > pos) list = up;
-        else if (lane == pos) list = x;
-        kth = __shfl_sync(kFull, list, k - 1);
-      }
-    }
-  }
-  return list;
-}
-
 __global__ void __launch_bounds__(256) k_knn_levels(
     const float2 *__restrict__ coords, int n, int k,
     const float *__restrict__ thr, int J, uint16_t *__restrict__ cand,
@@ -258,23 +223,28 @@ struct Visited {
       __syncwarp();
     }
   }
-  __device__ __forceinline__ bool test(int c) const {
-    if (V == 0) return (s[c >> 5] >> (c & 31)) & 1u;
-    const int src = (c >> 5) & 31;
-    uint32_t word = __shfl_sync(kFull, w0, src);
+  // Bitmap word holding node c (the shuffle source lane is taken modulo 32).
+  __device__ __forceinline__ uint32_t word_of(int c) const {
+    if (V == 0) return s[c >> 5];
+    uint32_t word = __shfl_sync(kFull, w0, c >> 5);
     if (V == 2) {
-      const uint32_t hi = __shfl_sync(kFull, w1, src);
+      const uint32_t hi = __shfl_sync(kFull, w1, c >> 5);
       word = (c >> 10) ? hi : word;
     }
-    return (word >> (c & 31)) & 1u;
+    return word;
+  }
+  __device__ __forceinline__ bool test(int c) const {
+    return (word_of(c) & (1u << (c & 31))) != 0u;
   }
   __device__ __forceinline__ void set(int node, int lane) {
     const uint32_t bit = 1u << (node & 31);
     if (V == 0) {
       if (lane == 0) s[node >> 5] |= bit;
       __syncwarp();
-    } else if (lane == ((node >> 5) & 31)) {
-      if (V == 2 && (node >> 10)) w1 |= bit; else w0 |= bit;
+    } else {
+      const bool mine = lane == ((node >> 5) & 31);
+      if (V == 2 && (node >> 10)) w1 |= mine ? bit : 0u;
+      else w0 |= mine ? bit : 0u;
     }
   }
 };
@@ -378,38 +348,60 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
     const int future = fut64 > 0x7fffffffLL ? 0x7fffffff : (int)fut64;
     int room = cap;
     bool tight = !UNIT && room < max_dem;
+    // Row of the current node; the next row's loads are issued as soon as the
+    // next node is known, ahead of this step's bookkeeping.
+    int c = 0, dc = 0;
+    uint32_t w = 0u;
+    if (lane < k) {
+      c = tb.cand[lane];
+      w = tb.weight(lane);
+    }
+    if (!UNIT) dc = tb.demand(c);
     // Every demand is >= 1, so rem_dem > future >= 0 implies remaining > 0.
     while (rem_dem > future && load < cap) {
-      const int base = cur * k;
-      int c = 0, dc = 1;
-      uint32_t w = 0u;
-      if (lane < k) {
-        c = tb.cand[base + lane];
-        w = tb.weight(base + lane);
-      }
-      if (!UNIT) dc = tb.demand(c);
       bool ok = !vis.test(c);
       if (!UNIT) ok = ok && (!tight || dc <= room);
       const uint32_t wv = ok ? w : 0u;
       const uint32_t denom = __reduce_add_sync(kFull, wv);
-      const uint32_t cum = warp_incl_scan(wv, lane);
       // cum * 2^24 >= r * denom  <=>  cum >= ceil(r * denom / 2^24)
       const uint32_t thr =
           (uint32_t)(((unsigned long long)r_next * denom + 0xFFFFFFull) >> kDrawBits);
-      const unsigned m = __ballot_sync(kFull, wv != 0u && cum >= thr);
-      const int src = m ? __ffs(m) - 1 : 0;
+      // Inclusive scan; lanes 0..7 hold their full prefix after three steps,
+      // and most draws land there, so the last two steps run only if needed.
+      uint32_t cum = wv;
+#pragma unroll
+      for (int o = 1; o < 8; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(kFull, cum, o);
+        if (lane >= o) cum += t;
+      }
+      unsigned msk = __ballot_sync(kFull, lane < 8 && wv != 0u && cum >= thr);
+      if (msk == 0u) {
+#pragma unroll
+        for (int o = 8; o < 32; o <<= 1) {
+          const uint32_t t = __shfl_up_sync(kFull, cum, o);
+          if (lane >= o) cum += t;
+        }
+        msk = __ballot_sync(kFull, wv != 0u && cum >= thr);
+      }
+      const int src = msk ? __ffs(msk) - 1 : 0;
       int next = __shfl_sync(kFull, c, src);
       int dn = UNIT ? 1 : __shfl_sync(kFull, dc, src);
       if (denom == 0u) {
         next = nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), room, tight, lane);
         if (next <= 0) break;
         dn = tb.demand(next);
-      } else {
-        ++d;
-        if ((d & 127u) == 0u) draw_refill(dbuf, d, a.seed, epoch, (uint32_t)ant, a.stream, lane);
-        r_next = dbuf[d & 127u];
       }
-      if (lane == 0) route[pos] = next;
+      {
+        const int base = next * k;
+        c = 0;
+        w = 0u;
+        if (lane < k) {
+          c = tb.cand[base + lane];
+          w = tb.weight(base + lane);
+        }
+        if (!UNIT) dc = tb.demand(c);
+      }
+      route[pos] = next;  // every lane stores the same value
       vis.set(next, lane);
       ++pos;
       --remaining;
@@ -418,6 +410,11 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       room = cap - load;
       tight = !UNIT && room < max_dem;
       cur = next;
+      if (denom != 0u) {
+        ++d;
+        if ((d & 127u) == 0u) draw_refill(dbuf, d, a.seed, epoch, (uint32_t)ant, a.stream, lane);
+        r_next = dbuf[d & 127u];
+      }
     }
     if (lane == 0) {
       route[pos] = 0;
@@ -836,142 +833,6 @@ cudaError_t launch_set_run_limit(DevState *st, int limit, cudaStream_t s) {
 // Evaporation + deposit
 // ===========================================================================
 
-// quantize_tau / dequantize_tau of the reference (aco_cuda_kernels.cu:25-45),
-// the same expressions so that the device math rounds identically.
-__device__ __forceinline__ float dequant(uint8_t q, float log_min, float log_step) {
-  return expf((float)q * log_step + log_min);
-}
-
-__device__ __forceinline__ uint8_t quant(float tau, float log_min,
-                                         float log_step, uint8_t q_min,
-                                         uint8_t q_max) {
-  if (tau <= 0.0f) return q_min;
-  float log_t = logf(tau);
-  float q_f = (log_t - log_min) / log_step;
-  if (q_f <= (float)q_min) return q_min;
-  if (q_f >= (float)q_max) return q_max;
-  return (uint8_t)roundf(q_f);
-}
-
-// One arc (u, c): new = quantize(dequantize(tau[u][c]) + dep), max-ed into
-// tau[u][c] and tau[c][u] (aco_cuda_kernels.cu:614-623).  The caller
-// guarantees that no other thread touches these two cells concurrently.
-__device__ __forceinline__ void deposit_arc(const PheromoneView &pv,
-                                            size_t stride, int u, int c,
-                                            float dep) {
-  uint8_t *fwd = pv.tau + (size_t)u * stride + c;
-  uint8_t *rev = pv.tau + (size_t)c * stride + u;
-  const uint8_t old = ld_cg_u8(fwd);
-  const uint8_t nq = quant(dequant(old, pv.log_min, pv.log_step) + dep,
-                           pv.log_min, pv.log_step, pv.q_min, pv.q_max);
-  if (nq > old) st_cg_u8(fwd, nq);
-  const uint8_t oldr = ld_cg_u8(rev);
-  if (nq > oldr) st_cg_u8(rev, nq);
-}
-
-// Deposit of one solution by one block.  Arcs of different routes touch
-// different cells, except the depot loop (0,0) of empty routes; inside a
-// route of >= 4 nodes all 2(len-1) cells are distinct too.  So: route
-// offsets are scanned into shared memory; the arcs of routes of >= 4 nodes
-// are dealt over all threads, each thread loading all its cells before it
-// stores any; a one-customer route [0 a 0] (whose two arcs share the cells
-// {0,a}) is walked by one thread in order, and all empty routes by thread 0
-// in vehicle order.  s_off holds K+1 ints, or is null for very large K
-// (then every thread walks the length list).
-__device__ void deposit_solution(const PheromoneView &pv, size_t stride,
-                                 const int *nodes, const int *lens, int K,
-                                 float dep, int *s_off) {
-  const int bd = (int)blockDim.x, tid = (int)threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5;
-  if (!s_off) {
-    int off = 0, base = 0;
-    for (int v = 0; v < K; ++v) {
-      const int len = lens[v];
-      const int owner = base % bd;
-      if (len >= 4) {
-        for (int t = (tid - owner + bd) % bd; t < len - 1; t += bd)
-          deposit_arc(pv, stride, nodes[off + t], nodes[off + t + 1], dep);
-      } else if (len == 3 && tid == owner) {
-        deposit_arc(pv, stride, nodes[off], nodes[off + 1], dep);
-        deposit_arc(pv, stride, nodes[off + 1], nodes[off + 2], dep);
-      } else if (len == 2 && tid == 0) {
-        deposit_arc(pv, stride, nodes[off], nodes[off + 1], dep);
-      }
-      off += len;
-      base += len > 1 ? len - 1 : 0;
-    }
-    return;
-  }
-  if (warp == 0) {
-    int carry = 0;
-    for (int b = 0; b < K; b += 32) {
-      const int v = b + lane;
-      const int len = v < K ? lens[v] : 0;
-      const int inc = (int)warp_incl_scan((uint32_t)len, lane);
-      if (v < K) s_off[v + 1] = carry + inc;
-      carry += __shfl_sync(kFull, inc, 31);
-    }
-    if (lane == 0) s_off[0] = 0;
-  }
-  __syncthreads();
-  const int total = s_off[K];
-  constexpr int kBatch = 4;
-  for (int j0 = tid; j0 < total; j0 += kBatch * bd) {
-    int us[kBatch], cs[kBatch];
-    bool valid[kBatch];
-#pragma unroll
-    for (int q = 0; q < kBatch; ++q) {
-      const int j = j0 + q * bd;
-      valid[q] = false;
-      us[q] = cs[q] = 0;
-      if (j < total) {
-        int lo = 0, hi = K;  // route v with s_off[v] <= j < s_off[v+1]
-        while (hi - lo > 1) {
-          const int mid = (lo + hi) >> 1;
-          if (s_off[mid] <= j) lo = mid; else hi = mid;
-        }
-        const int off = s_off[lo], len = s_off[lo + 1] - off;
-        if (len >= 4 && j > off) {
-          valid[q] = true;
-          us[q] = nodes[j - 1];
-          cs[q] = nodes[j];
-        }
-      }
-    }
-    uint8_t fq[kBatch], rq[kBatch];
-#pragma unroll
-    for (int q = 0; q < kBatch; ++q) {
-      fq[q] = rq[q] = 0;
-      if (valid[q]) {
-        fq[q] = ld_cg_u8(pv.tau + (size_t)us[q] * stride + cs[q]);
-        rq[q] = ld_cg_u8(pv.tau + (size_t)cs[q] * stride + us[q]);
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < kBatch; ++q) {
-      if (valid[q]) {
-        const uint8_t nq = quant(dequant(fq[q], pv.log_min, pv.log_step) + dep, pv.log_min,
-                                 pv.log_step, pv.q_min, pv.q_max);
-        if (nq > fq[q]) st_cg_u8(pv.tau + (size_t)us[q] * stride + cs[q], nq);
-        if (nq > rq[q]) st_cg_u8(pv.tau + (size_t)cs[q] * stride + us[q], nq);
-      }
-    }
-  }
-  for (int v = tid; v < K; v += bd) {
-    const int off = s_off[v];
-    if (s_off[v + 1] - off == 3) {
-      deposit_arc(pv, stride, nodes[off], nodes[off + 1], dep);
-      deposit_arc(pv, stride, nodes[off + 1], nodes[off + 2], dep);
-    }
-  }
-  if (tid == 0) {
-    for (int v = 0; v < K; ++v)
-      if (s_off[v + 1] - s_off[v] == 2) deposit_arc(pv, stride, 0, 0, dep);
-  }
-}
-
-constexpr int kDepositSmemRoutes = 4096;
-
 __device__ __forceinline__ uint32_t evap4(uint32_t x, uint32_t floor4,
                                           uint32_t delta4) {
   return __vsub4(__vmaxu4(x, floor4), delta4);
@@ -1039,11 +900,11 @@ __global__ void __launch_bounds__(512) k_evap_deposit(EvapArgs a) {
   const float dep_g = a.st ? a.st->dep_global : a.dep_global;
   extern __shared__ int s_off[];
   int *offs = (a.iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
-  deposit_solution(pv, stride_n, a.ab.routes + (size_t)best * a.iv.route_stride,
+  deposit_solution(pv, stride_n, CompactNodes{a.ab.routes + (size_t)best * a.iv.route_stride},
                    a.ab.lens + (size_t)best * a.iv.K, a.iv.K, dep_i, offs);
   __syncthreads();
   if (a.gbest_nodes) {
-    deposit_solution(pv, stride_n, a.gbest_nodes, a.gbest_lens, a.iv.K, dep_g, offs);
+    deposit_solution(pv, stride_n, CompactNodes{a.gbest_nodes}, a.gbest_lens, a.iv.K, dep_g, offs);
   }
   if (threadIdx.x == 0) *a.counter = 0u;
 }

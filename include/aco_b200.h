@@ -139,6 +139,40 @@ ACO_API int aco_b200_evaporate_deposit(aco_b200_ctx *ctx, int best_ant,
                                float dep_iter, const int *gbest_nodes,
                                const int *gbest_lens, float dep_global);
 
+/*
+ * Evaporation then deposit without any device allocation, for callers that
+ * cannot allocate device memory while they run: applications that reserve
+ * all device memory up front and give plugins only buffers they own (a
+ * framework's caching allocator, a service with a fixed memory budget), or
+ * real-time loops where cudaMalloc/cudaFree are off limits because they can
+ * synchronise the device and can fail under memory pressure.  No counterpart
+ * in the reference (its pheromone update allocates through its solver).
+ *
+ * Every argument is caller-owned device memory or a scalar: d_tau is the
+ * (n+1)^2 log-quantized matrix (row stride n+1, 16-byte aligned), updated
+ * in place; the
+ * iteration-best and (optional, both NULL to skip) global-best solutions are
+ * in compact form (K segments [0 c.. 0] back to back, K lengths); rho gives
+ * the evaporation step as in the reference (src/cuda/aco_cuda.cu:214-215).
+ * Same result as aco_b200_evaporate_deposit.
+ *
+ * The kernel's scratch is a fixed array in the library's device memory
+ * (16.6 KB per GPU), so K may be at most 4096 routes; larger K is rejected
+ * with ACO_ERR_INVALID_INPUT and a message on stderr.  Every call on a GPU
+ * shares that array: calls whose kernels overlap on the GPU race, so issue
+ * them on one stream or otherwise order them.  The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before capturing a stream into a CUDA graph.
+ */
+ACO_API int aco_b200_evaporate_deposit_noalloc(uint8_t *d_tau, int n, int K,
+                                               const int *d_iter_nodes,
+                                               const int *d_iter_lens,
+                                               float dep_iter,
+                                               const int *d_gbest_nodes,
+                                               const int *d_gbest_lens,
+                                               float dep_global, double rho,
+                                               void *cuda_stream);
+
 /* Library build information. */
 ACO_API const char *aco_b200_build_info(void);
 

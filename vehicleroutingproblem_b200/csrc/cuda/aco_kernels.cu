@@ -360,7 +360,9 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
     // Every demand is >= 1, so rem_dem > future >= 0 implies remaining > 0.
     while (rem_dem > future && load < cap) {
       bool ok = !vis.test(c);
-      if (!UNIT) ok = ok && (!tight || dc <= room);
+      // Demands only bind when the room left is below the largest demand;
+      // until then the speculative demand load stays off the step's chain.
+      if (!UNIT && tight) ok = ok && dc <= room;
       const uint32_t wv = ok ? w : 0u;
       const uint32_t denom = __reduce_add_sync(kFull, wv);
       // cum * 2^24 >= r * denom  <=>  cum >= ceil(r * denom / 2^24)
@@ -410,11 +412,11 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       room = cap - load;
       tight = !UNIT && room < max_dem;
       cur = next;
-      if (denom != 0u) {
-        ++d;
-        if ((d & 127u) == 0u) draw_refill(dbuf, d, a.seed, epoch, (uint32_t)ant, a.stream, lane);
-        r_next = dbuf[d & 127u];
-      }
+      // A draw is consumed only by a roulette selection (denom > 0).
+      d += (denom != 0u) ? 1u : 0u;
+      if ((d & 127u) == 0u && denom != 0u)
+        draw_refill(dbuf, d, a.seed, epoch, (uint32_t)ant, a.stream, lane);
+      r_next = dbuf[d & 127u];
     }
     if (lane == 0) {
       route[pos] = 0;

@@ -140,6 +140,62 @@ ACO_API int aco_b200_evaporate_deposit(aco_b200_ctx *ctx, int best_ant,
                                const int *gbest_lens, float dep_global);
 
 /*
+ * Batched solving: many independent instances in one persistent launch.
+ * Each block takes instances from a queue and runs all their epochs itself
+ * (weights, construction, best, evaporation, deposit), so instances of
+ * uneven size share the GPU without any host round trip.  Instance i is
+ * solved exactly as aco_b200_setup/aco_b200_run solve it with seed + i, the
+ * same ants, candidate length, parameters and epoch rules.  Coordinates and
+ * demands are packed: instance i occupies n[i] + 1 consecutive entries.
+ * No counterpart in the reference (it solves one instance per process).
+ */
+typedef struct aco_b200_batch aco_b200_batch;
+
+typedef struct {
+  int count;                  /* instances                                 */
+  const int *n;               /* [count] customers (k <= n <= 2046)        */
+  const int *K;               /* [count] vehicles                          */
+  const long long *capacity;  /* [count] in demand units                   */
+  const float *x, *y;         /* packed [sum(n[i] + 1)] host               */
+  const int *demand;          /* packed, NULL = unit demand                */
+  int ants;                   /* per instance; 0 selects 64                */
+  int cand_k;                 /* 0 selects 32                              */
+  double alpha, beta, rho, tau0, Q;
+  unsigned int seed;          /* instance i uses seed + i                  */
+  int epochs;                 /* epochs per instance                       */
+  int stagnation_epochs;      /* 0 = none                                  */
+  double min_rel_improvement;
+} aco_b200_batch_problem;
+
+/* Launch shape: lanes per ant (16: two ants per warp, needs cand_k <= 16;
+ * 32: one), ants per block, queue order (0: as given, 1: largest first). */
+typedef struct {
+  int lanes_per_ant;
+  int ants_per_block;
+  int order;
+} aco_b200_batch_tuning;
+
+ACO_API int aco_b200_batch_create(aco_b200_batch **out, int device);
+ACO_API int aco_b200_batch_destroy(aco_b200_batch *batch);
+ACO_API int aco_b200_batch_setup(aco_b200_batch *batch, const aco_b200_batch_problem *problem);
+ACO_API int aco_b200_batch_set_tuning(aco_b200_batch *batch, const aco_b200_batch_tuning *tuning);
+ACO_API int aco_b200_batch_get_tuning(aco_b200_batch *batch, aco_b200_batch_tuning *tuning);
+/* Times every candidate launch shape on `trial_epochs` epochs of the whole
+ * batch and keeps the fastest; per-trial ms through trial_ms. */
+ACO_API int aco_b200_batch_autotune(aco_b200_batch *batch, int trial_epochs,
+                                    aco_b200_batch_tuning *chosen, float *trial_ms,
+                                    int max_trials, int *n_trials);
+/* One launch solving every instance; _enqueue does not synchronise. */
+ACO_API int aco_b200_batch_solve(aco_b200_batch *batch);
+ACO_API int aco_b200_batch_enqueue(aco_b200_batch *batch);
+ACO_API int aco_b200_batch_synchronize(aco_b200_batch *batch);
+/* Best solution of one instance (compact form, as aco_b200_get_best). */
+ACO_API int aco_b200_batch_get(aco_b200_batch *batch, int instance, int *nodes, int *lens,
+                               double *cost, int *epochs);
+ACO_API int aco_b200_batch_get_costs(aco_b200_batch *batch, double *costs, int *epochs,
+                                     unsigned long long *steps);
+
+/*
  * Evaporation then deposit without any device allocation, for callers that
  * cannot allocate device memory while they run: applications that reserve
  * all device memory up front and give plugins only buffers they own (a

@@ -1,0 +1,77 @@
+"""GPU tests of the batched solver: every instance of a batch gives exactly
+what the single-instance solver gives with seed + i, whatever launch shape
+(lanes per ant, ants per block, queue order) runs it."""
+import numpy as np
+import pytest
+
+from vehicleroutingproblem_b200 import _native
+from vehicleroutingproblem_b200 import instances as I
+
+pytestmark = pytest.mark.gpu
+
+
+def mixed_instances():
+    out = []
+    for i, (n, K, dm) in enumerate([(20, 2, 30), (57, 3, 100), (140, 4, 100), (301, 6, 50),
+                                    (96, 2, 1), (233, 5, 100), (17, 3, 100), (480, 9, 100)]):
+        inst = I.uniform_instance(n, K, 950 + i, demand_max=max(dm, 1))
+        out.append(inst.unit_twin() if dm == 1 else inst)
+    out.append(I.clustered_instance(180, 4, 960))
+    return out
+
+
+def plain(inst, seed, ants, k, epochs, stagnation=0):
+    with _native.Context(0) as ctx:
+        ctx.setup_instance(inst, ants=ants, cand_k=k, seed=seed, fixed_epochs=epochs,
+                           stagnation_epochs=stagnation)
+        st = ctx.run(epochs)
+        nodes, lens, cost = ctx.best()
+        return nodes, lens, cost, st.epochs
+
+
+@pytest.fixture(scope="module")
+def reference_runs():
+    insts = mixed_instances()
+    return insts, [plain(inst, 500 + i, 16, 16, 12) for i, inst in enumerate(insts)]
+
+
+@pytest.mark.parametrize("tuning", [(32, 16, 1), (32, 8, 0), (16, 16, 1), (16, 32, 0), (32, 32, 1)])
+def test_batch_equals_single_instance_solver(reference_runs, tuning):
+    insts, ref = reference_runs
+    with _native.Batch(0) as b:
+        b.setup(insts, ants=16, cand_k=16, seed=500, epochs=12)
+        b.set_tuning(*tuning)
+        b.solve()
+        for i, (rn, rl, rc, re) in enumerate(ref):
+            nodes, lens, cost, ep = b.best(i)
+            assert ep == re == 12
+            assert cost == rc, (i, cost, rc)
+            assert np.array_equal(lens, rl) and np.array_equal(nodes, rn), i
+
+
+def test_batch_stagnation_rule_matches():
+    insts = mixed_instances()[:5]
+    ref = [plain(inst, 77 + i, 16, 16, 200, stagnation=4) for i, inst in enumerate(insts)]
+    with _native.Batch(0) as b:
+        b.setup(insts, ants=16, cand_k=16, seed=77, epochs=200, stagnation_epochs=4)
+        b.solve()
+        for i, (rn, rl, rc, re) in enumerate(ref):
+            nodes, lens, cost, ep = b.best(i)
+            assert ep == re and cost == rc and np.array_equal(nodes, rn)
+
+
+def test_autotune_keeps_results():
+    insts = I.batched_instances(24, seed0=31000)
+    with _native.Batch(0) as b:
+        b.setup(insts, ants=32, cand_k=16, seed=9, epochs=6)
+        chosen, ms = b.autotune(trial_epochs=2)
+        assert len(ms) >= 6 and (ms > 0).sum() >= 6
+        b.solve()
+        c1, e1, s1 = b.costs()
+        b.set_tuning(32, 16, 0)
+        b.solve()
+        c2, e2, s2 = b.costs()
+        assert np.array_equal(c1, c2) and np.array_equal(e1, e2) and np.array_equal(s1, s2)
+        assert np.all(e1 == 6) and np.all(np.isfinite(c1) | (c1 > 1e300))
+    for i in (0, 7, 23):
+        assert plain(insts[i], 9 + i, 32, 16, 6)[2] == c1[i]

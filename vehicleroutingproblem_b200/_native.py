@@ -32,7 +32,11 @@ EXPORTED = [
     "aco_b200_get_tau", "aco_b200_set_tau", "aco_b200_get_candidates",
     "aco_b200_get_tables", "aco_b200_get_weights", "aco_b200_construct",
     "aco_b200_get_ants", "aco_b200_evaporate_deposit", "aco_b200_build_info",
-    "aco_b200_profile_epochs",
+    "aco_b200_profile_epochs", "aco_b200_evaporate_deposit_noalloc",
+    "aco_b200_batch_create", "aco_b200_batch_destroy", "aco_b200_batch_setup",
+    "aco_b200_batch_set_tuning", "aco_b200_batch_get_tuning", "aco_b200_batch_autotune",
+    "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
+    "aco_b200_batch_get", "aco_b200_batch_get_costs",
     "aco_status_string", "aco_vrp_cuda_with_capacity", "aco_vrp_cuda_with_demands",
     "solution_create", "solution_free", "solution_reset", "solution_copy",
     "solution_cost", "route_append", "solution_validate",
@@ -112,6 +116,14 @@ def load():
         "aco_b200_get_ants": [vp, vp, vp, vp, vp, vp, vp],
         "aco_b200_evaporate_deposit": [vp, i32, f32, vp, vp, f32],
         "aco_b200_profile_epochs": [vp, i32, vp],
+        "aco_b200_batch_create": [vp, i32], "aco_b200_batch_destroy": [vp],
+        "aco_b200_batch_setup": [vp, vp], "aco_b200_batch_set_tuning": [vp, vp],
+        "aco_b200_batch_get_tuning": [vp, vp],
+        "aco_b200_batch_autotune": [vp, i32, vp, vp, i32, vp],
+        "aco_b200_batch_solve": [vp], "aco_b200_batch_enqueue": [vp],
+        "aco_b200_batch_synchronize": [vp],
+        "aco_b200_batch_get": [vp, i32, vp, vp, vp, vp],
+        "aco_b200_batch_get_costs": [vp, vp, vp, vp],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)
@@ -282,6 +294,123 @@ class Context:
         _check(self._lib.aco_b200_evaporate_deposit(self._h, best_ant, dep_iter, _p(gn),
                                                     _p(gl), dep_global),
                "aco_b200_evaporate_deposit")
+
+
+class BatchProblem(C.Structure):
+    _fields_ = [("count", C.c_int), ("n", C.c_void_p), ("K", C.c_void_p),
+                ("capacity", C.c_void_p), ("x", C.c_void_p), ("y", C.c_void_p),
+                ("demand", C.c_void_p), ("ants", C.c_int), ("cand_k", C.c_int),
+                ("alpha", C.c_double), ("beta", C.c_double), ("rho", C.c_double),
+                ("tau0", C.c_double), ("Q", C.c_double), ("seed", C.c_uint),
+                ("epochs", C.c_int), ("stagnation_epochs", C.c_int),
+                ("min_rel_improvement", C.c_double)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("lanes_per_ant", C.c_int), ("ants_per_block", C.c_int), ("order", C.c_int)]
+
+    def as_tuple(self):
+        return (self.lanes_per_ant, self.ants_per_block, self.order)
+
+
+class Batch:
+    """Many instances in one persistent launch (aco_b200_batch)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load()
+        self._h = C.c_void_p()
+        _check(self._lib.aco_b200_batch_create(C.byref(self._h), device), "aco_b200_batch_create")
+        self.count = 0
+        self.instances = []
+
+    def close(self):
+        if self._h:
+            self._lib.aco_b200_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def setup(self, instances, ants=64, cand_k=16, seed=1234, epochs=300,
+              stagnation_epochs=0, alpha=1.0, beta=2.0, rho=0.5, tau0=1.0, Q=1.0,
+              min_rel_improvement=1e-3):
+        ns = np.array([i.n for i in instances], np.int32)
+        Ks = np.array([i.vehicles for i in instances], np.int32)
+        caps = np.array([i.capacity for i in instances], np.int64)
+        x = np.concatenate([i.x for i in instances]).astype(np.float32)
+        y = np.concatenate([i.y for i in instances]).astype(np.float32)
+        unit = all(i.is_unit_demand() for i in instances)
+        d = None if unit else np.concatenate([i.demand for i in instances]).astype(np.int32)
+        self._keep = [ns, Ks, caps, x, y, d]
+        p = BatchProblem(count=len(instances), n=_p(ns).value, K=_p(Ks).value,
+                         capacity=_p(caps).value, x=_p(x).value, y=_p(y).value,
+                         demand=None if d is None else _p(d).value, ants=ants, cand_k=cand_k,
+                         alpha=alpha, beta=beta, rho=rho, tau0=tau0, Q=Q,
+                         seed=seed & 0xffffffff, epochs=epochs,
+                         stagnation_epochs=stagnation_epochs,
+                         min_rel_improvement=min_rel_improvement)
+        _check(self._lib.aco_b200_batch_setup(self._h, C.byref(p)), "aco_b200_batch_setup")
+        self.count = len(instances)
+        self.instances = list(instances)
+        return self
+
+    def set_tuning(self, lanes_per_ant, ants_per_block, order=1):
+        t = BatchTuning(lanes_per_ant, ants_per_block, order)
+        _check(self._lib.aco_b200_batch_set_tuning(self._h, C.byref(t)),
+               "aco_b200_batch_set_tuning")
+
+    def tuning(self):
+        t = BatchTuning()
+        _check(self._lib.aco_b200_batch_get_tuning(self._h, C.byref(t)),
+               "aco_b200_batch_get_tuning")
+        return t.as_tuple()
+
+    def autotune(self, trial_epochs=3):
+        t = BatchTuning()
+        ms = np.zeros(16, np.float32)
+        nt = C.c_int()
+        _check(self._lib.aco_b200_batch_autotune(self._h, trial_epochs, C.byref(t), _p(ms), 16,
+                                                 C.byref(nt)), "aco_b200_batch_autotune")
+        return t.as_tuple(), ms[: nt.value].copy()
+
+    def solve(self):
+        _check(self._lib.aco_b200_batch_solve(self._h), "aco_b200_batch_solve")
+
+    def enqueue(self):
+        _check(self._lib.aco_b200_batch_enqueue(self._h), "aco_b200_batch_enqueue")
+
+    def synchronize(self):
+        _check(self._lib.aco_b200_batch_synchronize(self._h), "aco_b200_batch_synchronize")
+
+    def best(self, i):
+        inst = self.instances[i]
+        nodes = np.zeros(inst.n + 2 * inst.vehicles, np.int32)
+        lens = np.zeros(inst.vehicles, np.int32)
+        cost = C.c_double()
+        ep = C.c_int()
+        rc = self._lib.aco_b200_batch_get(self._h, i, _p(nodes), _p(lens), C.byref(cost),
+                                          C.byref(ep))
+        if rc == ACO_ERR_NO_SOLUTION:
+            return nodes[:0], lens, float("inf"), ep.value
+        _check(rc, "aco_b200_batch_get")
+        return nodes[: int(lens.sum())].copy(), lens, cost.value, ep.value
+
+    def costs(self):
+        c = np.zeros(self.count, np.float64)
+        e = np.zeros(self.count, np.int32)
+        s = np.zeros(self.count, np.uint64)
+        _check(self._lib.aco_b200_batch_get_costs(self._h, _p(c), _p(e), _p(s)),
+               "aco_b200_batch_get_costs")
+        return c, e, s
 
 
 def build_info() -> str:

@@ -1,30 +1,36 @@
 """Benchmark of the ACO-for-CVRP hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload n1000|small|clustered2000|batched]
 
-A step is one ACO epoch (construct all ants, iteration/global best, evaporate,
-deposit) over the n=1000, K=8 workload: uniform integer coordinates in
+Default workload (n1000): n=1000, K=8 uniform integer coordinates in
 [0,1000]^2 from seed 19001, depot (500,500), demands uniform in [1,100],
-Q = ceil(sum(d)/(0.9 K)), 256 ants, 32-NN candidate lists.  The metric is
-ant-steps/s (one ant-step = one customer move or depot return).
+Q = ceil(sum(d)/(0.9 K)), 256 ants, 32-NN candidate lists.  A step is one
+ACO epoch (construct all ants, iteration/global best, evaporate, deposit);
+the metric is ant-steps/s (one ant-step = one customer move or depot return).
+small: n=100, K=4, demands [1,30], seed 1001, 128 ants, 20-NN.
+clustered2000: n=2000, K=16, 70% in 8 Gaussian clusters, 1024 ants, 32-NN.
+batched: 512 instances (n~U[50,500], K=ceil(n/60), seeds 30000-30511), 64
+ants, 16-NN, 300 epochs each, all in one persistent launch; a step is one
+solve of the whole batch and the metric is instances/s.
 
-* value: device time of K epochs (CUDA events on the library's stream, the L2
-  flushed by a 256 MiB write between epochs outside the events), all ranks'
-  ant-steps over the max-over-ranks time.
-* e2e: the same metric through the public C ABI with host buffers: per step
-  one solve (upload of coordinates and demands, candidate lists, 64 epochs,
-  download of the best routes and cost), timed on the host.
-* roofline: the construct kernel (the dominant one), algorithmic bytes per
-  ant-step k(4 + 4 + 1) (candidate id, weight, pheromone byte), over its mean
-  event-timed duration.
+* value: device time (CUDA events on the library's stream), L2 flushed by a
+  256 MiB write between steps outside the events, all ranks' work over the
+  max-over-ranks time.
+* e2e: the same metric through the public C ABI with host buffers (per step
+  one solve: upload, candidate lists, epochs, download of the result), timed
+  on the host.
+* roofline: the dominant kernel, algorithmic bytes per ant-step k(4 + 4 + 1)
+  (candidate id, weight, pheromone byte) over its mean event-timed duration.
 * cpu_baseline / --impl reference: the reference's OpenMP solver
   (oracle/_ref/aco_vrp_omp.out, built from the reference sources) on the
-  unit-demand twin of the workload with all host threads, fixed epochs; the
-  oracle port (single thread) if that build is absent.
+  unit-demand twins with all host threads and fixed epochs; the oracle port
+  (single thread) if that build is absent.
 
-Multi-GPU (torchrun, one rank per GPU): every rank runs its own colony of 256
-ants on the same instance with its own seed (weak scaling); the timed region
-has no collective.
+Multi-GPU (torchrun, one rank per GPU): every rank solves its own share --
+a colony of its own on the same instance (single-instance workloads) or its
+own slice of the instances (batched) -- with no collective in the timed
+region (weak scaling for colonies, strong for the batch).
 """
 from __future__ import annotations
 
@@ -45,14 +51,22 @@ sys.path.insert(0, ROOT)
 
 from vehicleroutingproblem_b200 import instances as I  # noqa: E402
 
-WORKLOAD = dict(name="n1000 K8 uniform seed19001 demand[1,100] 256 ants 32-NN",
-                ants=256, cand_k=32)
-E2E_EPOCHS = 64
-BYTES_PER_ANT_STEP = 32 * (4 + 4 + 1)
+WORKLOADS = {
+    "n1000": dict(factory=I.workload_n1000, ants=256, cand_k=32, e2e_epochs=64,
+                  name="n1000 K8 uniform seed19001 demand[1,100] 256 ants 32-NN"),
+    "small": dict(factory=I.workload_small, ants=128, cand_k=20, e2e_epochs=200,
+                  name="n100 K4 uniform seed1001 demand[1,30] 128 ants 20-NN"),
+    "clustered2000": dict(factory=I.workload_clustered2000, ants=1024, cand_k=32, e2e_epochs=32,
+                          name="n2000 K16 clustered seed29001 demand[1,100] 1024 ants 32-NN"),
+}
+BATCHED = dict(count=512, seed0=30000, ants=64, cand_k=16, epochs=300,
+               name="512 instances n~U[50,500] K=ceil(n/60) seeds 30000-30511 demand[1,100] "
+                    "64 ants 16-NN 300 epochs")
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_construct launch on
-# this workload (profiles/k_construct_n1000.md): the candidate tables come
-# from L2 into shared memory, so DRAM sees little of the algorithmic bytes.
-CONSTRUCT_DRAM_BYTES_PER_LAUNCH = 234496
+# the n1000 workload (profiles/k_construct_n1000.md): the candidate tables
+# come from L2 into shared memory, so DRAM sees little of the algorithmic
+# bytes.  Other workloads report null.
+CONSTRUCT_DRAM_BYTES_PER_LAUNCH = {"n1000": 234496}
 OMP_BIN = os.path.join(ROOT, "oracle", "_ref", "aco_vrp_omp.out")
 
 
@@ -85,6 +99,7 @@ class ClockSampler:
                 ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            time.sleep(0.5)  # let the sampler start before the timed region
         return self
 
     def __exit__(self, *a):
@@ -127,7 +142,7 @@ def dist_env():
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference's OpenMP solver on the unit-demand twin
+# CPU baseline: the reference's OpenMP solver on unit-demand twins
 # ---------------------------------------------------------------------------
 
 def _omp_run(vrp_path, K, ants, epochs, threads):
@@ -142,23 +157,27 @@ def _omp_run(vrp_path, K, ants, epochs, threads):
     return dt
 
 
-def cpu_baseline(inst, ants, target_s=12.0):
+def _omp_epoch_seconds(inst, ants, threads, target_s, td):
+    """Seconds per epoch of the reference OpenMP solver, set-up excluded."""
+    path = os.path.join(td, inst.name + ".vrp")
+    I.write_vrp(inst.unit_twin(), path)
+    t1 = _omp_run(path, inst.vehicles, ants, 2, threads)
+    t2 = _omp_run(path, inst.vehicles, ants, 6, threads)
+    per = max((t2 - t1) / 4.0, 1e-6)
+    epochs = int(max(4, min(400, target_s / per)))
+    ta = _omp_run(path, inst.vehicles, ants, 2, threads)
+    tb = _omp_run(path, inst.vehicles, ants, 2 + epochs, threads)
+    return max((tb - ta) / epochs, 1e-9), epochs
+
+
+def cpu_baseline(inst, ants, target_s=12.0, cand_k=32):
     """ant-steps/s of the reference's own CPU path, bounded sample."""
     n, K = inst.n, inst.vehicles
     steps_per_epoch = ants * (n + K)
     if os.path.exists(OMP_BIN):
         threads = os.cpu_count() or 1
-        twin = inst.unit_twin()
         with tempfile.TemporaryDirectory() as td:
-            path = os.path.join(td, "twin.vrp")
-            I.write_vrp(twin, path)
-            t1 = _omp_run(path, K, ants, 2, threads)
-            t2 = _omp_run(path, K, ants, 6, threads)
-            per_epoch = max((t2 - t1) / 4.0, 1e-6)
-            epochs = int(max(4, min(400, target_s / per_epoch)))
-            ta = _omp_run(path, K, ants, 2, threads)
-            tb = _omp_run(path, K, ants, 2 + epochs, threads)
-            per_epoch = max((tb - ta) / epochs, 1e-9)
+            per_epoch, epochs = _omp_epoch_seconds(inst, ants, threads, target_s, td)
         return {"value": steps_per_epoch / per_epoch, "unit": "ant-steps/s", "cores": threads,
                 "kind": "reference",
                 "sample": (f"reference OpenMP solver (aco_parallel.c, no MPI) on the unit-demand "
@@ -168,36 +187,66 @@ def cpu_baseline(inst, ants, target_s=12.0):
     from oracle import oracle as O
     O.build()
     A, lut, thr = O.tables()
-    k = WORKLOAD["cand_k"]
-    cand = O.knn(inst.x, inst.y, k)
-    lvl = O.levels(inst.x, inst.y, cand, k, thr)
+    cand = O.knn(inst.x, inst.y, cand_k)
+    lvl = O.levels(inst.x, inst.y, cand, cand_k, thr)
     tau = np.full((n + 1) ** 2, O.params()["q_tau0"], np.uint8)
-    w = O.weights(n, k, cand, lvl, tau, A, lut)
+    w = O.weights(n, cand_k, cand, lvl, tau, A, lut)
     t0 = time.perf_counter()
     steps = 0
     for a in range(ants):
-        steps += O.construct_ant(inst.x, inst.y, inst.demand, K, inst.capacity, k, cand, w,
-                                 1234, 0, a)[4]
+        steps += O.construct_ant(inst.x, inst.y, inst.demand, K, inst.capacity, cand_k, cand,
+                                 w, 1234, 0, a)[4]
     dt = time.perf_counter() - t0
     return {"value": steps / dt, "unit": "ant-steps/s", "cores": 1, "kind": "port",
             "sample": f"oracle construct of {ants} ants, one epoch, one thread"}
 
 
+def cpu_baseline_batched(insts, target_s=15.0):
+    """instances/s of the reference OpenMP solver over a sample of the batch
+    (each instance: its own process, 64 ants, 300 fixed epochs), scaled to the
+    whole batch by work (n + K)."""
+    if not os.path.exists(OMP_BIN):
+        return {"error": "oracle/_ref not built"}
+    threads = os.cpu_count() or 1
+    spent, idx = 0.0, []
+    with tempfile.TemporaryDirectory() as td:
+        for i in range(0, len(insts), max(1, len(insts) // 32)):
+            per_epoch, _ = _omp_epoch_seconds(insts[i], BATCHED["ants"], threads, 0.5, td)
+            spent += per_epoch * BATCHED["epochs"]
+            idx.append(i)
+            if spent > target_s:
+                break
+    w = np.array([x.n + x.vehicles for x in insts], float)
+    total = spent * w.sum() / w[idx].sum()
+    return {"value": len(insts) / total, "unit": "instances/s", "cores": threads,
+            "kind": "reference",
+            "sample": (f"reference OpenMP solver on the unit-demand twins of {len(idx)} of the "
+                       f"{len(insts)} instances, 64 ants, per-epoch time x 300 epochs, scaled "
+                       f"to the batch by n+K, OMP_NUM_THREADS={threads}")}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
-    inst = I.workload_n1000()
-    cb = cpu_baseline(inst, WORKLOAD["ants"], target_s=max(4.0, 3.0 * args.steps))
-    line = {"impl": "reference", "metric": "ant-steps/s", "value": cb["value"],
-            "unit": "ant-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "data": "synthetic",
-            "config": {"workload": WORKLOAD["name"], "n": inst.n, "K": inst.vehicles,
-                       "ants": WORKLOAD["ants"], "cand_k": WORKLOAD["cand_k"],
-                       "note": "reference CPU path runs the unit-demand twin (its parser "
-                               "accepts demand 1 only)"},
-            "cpu_baseline": cb,
-            "e2e": {"value": cb["value"], "unit": "ant-steps/s", "h2d_bytes_per_step": 0,
+    if args.workload == "batched":
+        insts = I.batched_instances(BATCHED["count"], BATCHED["seed0"])
+        cb = cpu_baseline_batched(insts)
+        cfg = {"workload": BATCHED["name"], "instances": BATCHED["count"]}
+        metric, unit = "instances/s", "instances/s"
+    else:
+        wl = WORKLOADS[args.workload]
+        inst = wl["factory"]()
+        cb = cpu_baseline(inst, wl["ants"], target_s=max(4.0, min(20.0, 0.01 * args.steps)),
+                          cand_k=wl["cand_k"])
+        cfg = {"workload": wl["name"], "n": inst.n, "K": inst.vehicles, "ants": wl["ants"],
+               "cand_k": wl["cand_k"]}
+        metric, unit = "ant-steps/s", "ant-steps/s"
+    cfg["note"] = "reference CPU path runs the unit-demand twins (its parser accepts demand 1 only)"
+    line = {"impl": "reference", "metric": metric, "value": cb.get("value"), "unit": unit,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "data": "synthetic", "config": cfg, "cpu_baseline": cb,
+            "e2e": {"value": cb.get("value"), "unit": unit, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -207,31 +256,24 @@ def run_reference_arm(args, rank, world):
 # GPU arm
 # ---------------------------------------------------------------------------
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=8)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    args = ap.parse_args()
-    args.warmup = max(args.warmup, 3)
-    rank, world, local = dist_env()
+def timed_steps(torch, stream, steps, enqueue, flush):
+    """Device ms of `steps` calls of enqueue(), each bracketed by events, the
+    L2 flushed between steps outside the events."""
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    for i in range(steps):
+        flush.fill_(i & 0xff)
+        evs[i][0].record(stream)
+        enqueue()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs)
 
-    if args.impl == "reference":
-        return run_reference_arm(args, rank, world)
 
-    import torch
-    import torch.distributed as dist
-    from vehicleroutingproblem_b200 import _native
-
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-
-    inst = I.workload_n1000()
-    n, K, m, k = inst.n, inst.vehicles, WORKLOAD["ants"], WORKLOAD["cand_k"]
+def run_single(args, rank, world, local, torch, dist, _native):
+    wl = WORKLOADS[args.workload]
+    inst = wl["factory"]()
+    n, K, m, k = inst.n, inst.vehicles, wl["ants"], wl["cand_k"]
     # A dedicated stream (the default stream's handle is 0, which the C ABI
     # reads as "use your own stream"): the library's kernels, the L2 flush and
     # the timing events all go to it.
@@ -240,57 +282,41 @@ def main():
     ctx = _native.Context(local)
     ctx.set_stream(stream.cuda_stream)
     ctx.setup_instance(inst, ants=m, cand_k=k, seed=1234 + 7919 * rank)
-
     ctx.enqueue_epochs(args.warmup)
     torch.cuda.synchronize()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     steps0 = ctx.state().total_steps
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
-        time.sleep(0.5)  # let the sampler start before the timed region
         wall0 = time.perf_counter()
-        for i in range(args.steps):
-            flush.fill_(i & 0xff)
-            evs[i][0].record(stream)
-            ctx.enqueue_epochs(1)
-            evs[i][1].record(stream)
-        torch.cuda.synchronize()
+        dev_ms = timed_steps(torch, stream, args.steps, lambda: ctx.enqueue_epochs(1), flush)
         wall = time.perf_counter() - wall0
     if world > 1:
         dist.barrier()
-    dev_ms = sum(a.elapsed_time(b) for a, b in evs)
     st = ctx.state()
     steps_done = st.total_steps - steps0
     assert st.error == 0 and st.epochs == args.warmup + args.steps
-
-    # Per-kernel device times (event between every kernel), for the roofline.
     kms = ctx.profile_epochs(32) / 32.0
     t = torch.tensor([dev_ms, float(steps_done)], dtype=torch.float64, device="cuda")
     if world > 1:
-        tmax = t.clone()
-        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(tmax[1:2], op=dist.ReduceOp.SUM)
-        t = tmax
+        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
     dev_ms_max, steps_all = float(t[0]), float(t[1])
     value = steps_all / (dev_ms_max / 1e3)
 
-    # End to end through the public API with host buffers.
     e2e_vals = []
     h2d = (n + 1) * (8 + 4) + 4095 * 4 + 2 * 256 * 4
     d2h = (n + 2 * K) * 4 + K * 4
     for i in range(args.e2e_steps):
         t0 = time.perf_counter()
         with _native.Context(local) as c2:
-            c2.setup_instance(inst, ants=m, cand_k=k, seed=99 + i, fixed_epochs=E2E_EPOCHS)
-            s2 = c2.run(E2E_EPOCHS)
+            c2.setup_instance(inst, ants=m, cand_k=k, seed=99 + i, fixed_epochs=wl["e2e_epochs"])
+            s2 = c2.run(wl["e2e_epochs"])
             c2.best()
         dt = time.perf_counter() - t0
-        if i > 0:  # first call pays the one-time module load
+        if i > 0:  # the first call pays the one-time module load
             e2e_vals.append(s2.total_steps / dt)
     e2e = statistics.median(e2e_vals) if e2e_vals else None
     if world > 1:
@@ -299,12 +325,10 @@ def main():
         e2e = float(te[0])
 
     peak, peak_kind = load_peaks()
-    construct_s = float(kms[1]) / 1e3
-    steps_per_launch = steps_done / args.steps
-    achieved = BYTES_PER_ANT_STEP * steps_per_launch / construct_s / 1e9
+    bytes_per_step = k * (4 + 4 + 1)
+    achieved = bytes_per_step * (steps_done / args.steps) / (float(kms[1]) / 1e3) / 1e9
     total_k = float(kms.sum())
-    clocks = clk.summary()
-
+    line = None
     if rank == 0:
         line = {
             "metric": "ant-steps/s", "value": value, "unit": "ant-steps/s", "n_gpus": world,
@@ -313,34 +337,193 @@ def main():
             "scaling": "weak", "vs_baseline": None,
             "dtype": "int32 weights + u8 pheromone (f64 route costs)",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD["name"], "n": n, "K": K, "capacity": inst.capacity,
+            "config": {"workload": wl["name"], "n": n, "K": K, "capacity": inst.capacity,
                        "ants": m, "cand_k": k, "step": "one epoch",
                        "l2": "flushed between timed steps (256 MiB write outside the events)",
-                       "parallelism": f"{world} independent colonies" if world > 1 else "1 GPU"},
+                       "parallelism": f"{world} colonies, one per GPU" if world > 1 else "1 GPU"},
             "wall_s": wall,
             "gpu_launches": 4 * args.steps,
             "kernels_us": {"weights": float(kms[0]) * 1e3, "construct": float(kms[1]) * 1e3,
                            "best": float(kms[2]) * 1e3, "evap_deposit": float(kms[3]) * 1e3},
             "kernel_share": {"construct": float(kms[1]) / total_k if total_k else None},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": CONSTRUCT_DRAM_BYTES_PER_LAUNCH,
+                         "frac": achieved / peak,
+                         "traffic": CONSTRUCT_DRAM_BYTES_PER_LAUNCH.get(args.workload),
                          "kernel": "k_construct", "peak_kind": peak_kind,
-                         "bytes_per_ant_step": BYTES_PER_ANT_STEP},
+                         "bytes_per_ant_step": bytes_per_step},
             "e2e": {"value": e2e, "unit": "ant-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
-                    "step": f"one solve through the C ABI: upload, candidates, {E2E_EPOCHS} "
+                    "step": f"one solve through the C ABI: upload, candidates, {wl['e2e_epochs']} "
                             "epochs, download of the best routes"},
-            "clocks": clocks,
+            "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:
             try:
-                line["cpu_baseline"] = cpu_baseline(inst, m)
+                line["cpu_baseline"] = cpu_baseline(inst, m, cand_k=k)
             except Exception as exc:  # reported, not fatal
                 line["cpu_baseline"] = {"error": str(exc)[:200]}
-        print(json.dumps(line), flush=True)
     ctx.close()
+    return line
+
+
+def run_batched(args, rank, world, local, torch, dist, _native):
+    insts_all = I.batched_instances(BATCHED["count"], BATCHED["seed0"])
+    mine = list(range(rank, len(insts_all), world))  # this rank's slice
+    insts = [insts_all[i] for i in mine]
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    b = _native.Batch(local)
+    b.set_stream(stream.cuda_stream)
+    b.setup(insts, ants=BATCHED["ants"], cand_k=BATCHED["cand_k"], seed=BATCHED["seed0"],
+            epochs=BATCHED["epochs"])
+    chosen, trials = b.autotune(trial_epochs=3)
+    for _ in range(args.warmup):
+        b.enqueue()
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     if world > 1:
-        dist.destroy_process_group()
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        wall0 = time.perf_counter()
+        dev_ms = timed_steps(torch, stream, args.steps, b.enqueue, flush)
+        wall = time.perf_counter() - wall0
+    if world > 1:
+        dist.barrier()
+    costs, epochs, steps = b.costs()
+    assert np.all(epochs == BATCHED["epochs"])
+    t = torch.tensor([dev_ms, float(len(insts)), float(steps.sum())], dtype=torch.float64,
+                     device="cuda")
+    if world > 1:
+        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:3], op=dist.ReduceOp.SUM)
+    dev_ms_max, count_all, steps_all = float(t[0]), float(t[1]), float(t[2])
+    value = count_all * args.steps / (dev_ms_max / 1e3)
+    ant_steps_s = steps_all * args.steps / (dev_ms_max / 1e3)
+
+    # End to end through the C ABI with host buffers: set-up (upload, k-NN),
+    # one solve, download of all costs and best routes.
+    e2e_vals = []
+    for i in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        with _native.Batch(local) as b2:
+            b2.setup(insts, ants=BATCHED["ants"], cand_k=BATCHED["cand_k"],
+                     seed=BATCHED["seed0"], epochs=BATCHED["epochs"])
+            b2.set_tuning(*chosen)
+            b2.solve()
+            b2.costs()
+            for j in range(len(insts)):
+                b2.best(j)
+        dt = time.perf_counter() - t0
+        if i > 0:
+            e2e_vals.append(len(insts) / dt)
+    e2e = statistics.median(e2e_vals) if e2e_vals else None
+    if world > 1:
+        te = torch.tensor([e2e or 0.0], dtype=torch.float64, device="cuda")
+        dist.all_reduce(te, op=dist.ReduceOp.SUM)
+        e2e = float(te[0])
+    nodes = sum(x.n + 1 for x in insts)
+    h2d = nodes * 16 + len(insts) * 24 + 4095 * 4
+    d2h = len(insts) * (8 + 4 + 8) + sum((x.n + 3 * x.vehicles) * 4 + 12 for x in insts)
+
+    # Looping the single-instance solver over a sample, scaled by work.
+    looped = None
+    if rank == 0 and args.looped_sample > 0:
+        sample = list(range(0, len(insts), max(1, len(insts) // args.looped_sample)))
+        t0 = time.perf_counter()
+        for i in sample:
+            with _native.Context(local) as ctx:
+                ctx.setup_instance(insts[i], ants=BATCHED["ants"], cand_k=BATCHED["cand_k"],
+                                   seed=BATCHED["seed0"] + mine[i], fixed_epochs=BATCHED["epochs"])
+                ctx.run(BATCHED["epochs"])
+                ctx.best()
+        ts = time.perf_counter() - t0
+        w = np.array([x.n + x.vehicles for x in insts], float)
+        t_all = ts * w.sum() / w[sample].sum()
+        looped = {"value": len(insts) / t_all, "unit": "instances/s",
+                  "sample": f"{len(sample)} instances solved one after another with the "
+                            "single-instance C ABI (300 epochs each), scaled by n+K"}
+    line = None
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        bytes_per_step = BATCHED["cand_k"] * (4 + 4 + 1)
+        achieved = bytes_per_step * ant_steps_s / 1e9
+        line = {
+            "metric": "instances/s", "value": value, "unit": "instances/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None,
+            "dtype": "int32 weights + u8 pheromone (f64 route costs)", "data": "synthetic",
+            "config": {"workload": BATCHED["name"], "instances": BATCHED["count"],
+                       "step": "one solve of the whole batch (one persistent launch)",
+                       "tuning": {"lanes_per_ant": chosen[0], "ants_per_block": chosen[1],
+                                  "order": "largest first" if chosen[2] else "as given"},
+                       "autotune_trial_ms": [round(float(x), 3) for x in trials],
+                       "l2": "flushed between timed steps (256 MiB write outside the events)",
+                       "parallelism": f"instances split over {world} GPUs" if world > 1 else "1 GPU"},
+            "ant_steps_per_s": ant_steps_s,
+            "wall_s": wall, "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "k_batch_solve",
+                         "peak_kind": peak_kind, "bytes_per_ant_step": bytes_per_step},
+            "e2e": {"value": e2e, "unit": "instances/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "step": "set-up of the batch through the C ABI, one solve, download of "
+                            "every cost and best route"},
+            "looped_single_instance": looped,
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                line["cpu_baseline"] = cpu_baseline_batched(insts)
+            except Exception as exc:
+                line["cpu_baseline"] = {"error": str(exc)[:200]}
+    b.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=None)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="n1000",
+                    choices=sorted(WORKLOADS) + ["batched"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--looped-sample", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    batched = args.workload == "batched"
+    if args.steps is None:
+        args.steps = 3 if batched else 2000
+    if args.warmup is None:
+        args.warmup = 3 if batched else 20
+    if args.e2e_steps is None:
+        args.e2e_steps = 3 if batched else 8
+    args.warmup = max(args.warmup, 3)
+    rank, world, local = dist_env()
+
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    from vehicleroutingproblem_b200 import _native
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        fn = run_batched if batched else run_single
+        line = fn(args, rank, world, local, torch, dist, _native)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
     return 0
 
 

@@ -177,6 +177,8 @@ typedef struct {
 
 ACO_API int aco_b200_batch_create(aco_b200_batch **out, int device);
 ACO_API int aco_b200_batch_destroy(aco_b200_batch *batch);
+/* Use an external stream; NULL = own. */
+ACO_API int aco_b200_batch_set_stream(aco_b200_batch *batch, void *cuda_stream);
 ACO_API int aco_b200_batch_setup(aco_b200_batch *batch, const aco_b200_batch_problem *problem);
 ACO_API int aco_b200_batch_set_tuning(aco_b200_batch *batch, const aco_b200_batch_tuning *tuning);
 ACO_API int aco_b200_batch_get_tuning(aco_b200_batch *batch, aco_b200_batch_tuning *tuning);

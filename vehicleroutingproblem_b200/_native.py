@@ -34,6 +34,7 @@ EXPORTED = [
     "aco_b200_get_ants", "aco_b200_evaporate_deposit", "aco_b200_build_info",
     "aco_b200_profile_epochs", "aco_b200_evaporate_deposit_noalloc",
     "aco_b200_batch_create", "aco_b200_batch_destroy", "aco_b200_batch_setup",
+    "aco_b200_batch_set_stream",
     "aco_b200_batch_set_tuning", "aco_b200_batch_get_tuning", "aco_b200_batch_autotune",
     "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
     "aco_b200_batch_get", "aco_b200_batch_get_costs",
@@ -117,6 +118,7 @@ def load():
         "aco_b200_evaporate_deposit": [vp, i32, f32, vp, vp, f32],
         "aco_b200_profile_epochs": [vp, i32, vp],
         "aco_b200_batch_create": [vp, i32], "aco_b200_batch_destroy": [vp],
+        "aco_b200_batch_set_stream": [vp, vp],
         "aco_b200_batch_setup": [vp, vp], "aco_b200_batch_set_tuning": [vp, vp],
         "aco_b200_batch_get_tuning": [vp, vp],
         "aco_b200_batch_autotune": [vp, i32, vp, vp, i32, vp],
@@ -362,6 +364,10 @@ class Batch:
         self.count = len(instances)
         self.instances = list(instances)
         return self
+
+    def set_stream(self, stream_handle: int) -> None:
+        _check(self._lib.aco_b200_batch_set_stream(self._h, C.c_void_p(stream_handle)),
+               "aco_b200_batch_set_stream")
 
     def set_tuning(self, lanes_per_ant, ants_per_block, order=1):
         t = BatchTuning(lanes_per_ant, ants_per_block, order)

@@ -602,6 +602,7 @@ int occupancy_batch(int threads, size_t smem) {
 struct aco_b200_batch {
   int device = 0, num_sms = 148;
   cudaStream_t stream = nullptr;
+  bool own_stream = true;
   bool ready = false;
   int count = 0, m = 0, k = 0, epochs = 0, max_rows = 0, max_K = 0, max_n = 0;
   BatchArgs args = {};
@@ -676,8 +677,22 @@ int aco_b200_batch_destroy(aco_b200_batch *b) {
   if (!b) return ACO_OK;
   cudaSetDevice(b->device);
   b->free_all();
-  if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
   delete b;
+  return ACO_OK;
+}
+
+int aco_b200_batch_set_stream(aco_b200_batch *b, void *cuda_stream) {
+  if (!b) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(b->device);
+  if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
+  if (cuda_stream) {
+    b->stream = (cudaStream_t)cuda_stream;
+    b->own_stream = false;
+  } else {
+    BTRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    b->own_stream = true;
+  }
   return ACO_OK;
 }
 

@@ -27,10 +27,14 @@ solve of the whole batch and the metric is instances/s.
   unit-demand twins with all host threads and fixed epochs; the oracle port
   (single thread) if that build is absent.
 
-Multi-GPU (torchrun, one rank per GPU): every rank solves its own share --
-a colony of its own on the same instance (single-instance workloads) or its
-own slice of the instances (batched) -- with no collective in the timed
-region (weak scaling for colonies, strong for the batch).
+Multi-GPU (torchrun, one rank per GPU).  Single-instance workloads split
+one colony over the ranks (vehicleroutingproblem_b200.sharding): every rank
+builds its own m ants on a replicated pheromone matrix, and each epoch ends
+with one NCCL all-gather of the ranks' best-ant packets, after which every
+rank applies the same deposits -- N ranks run one colony of N m ants (weak
+scaling: the ants per GPU stay fixed).  `--colony sharded` takes that path on
+one GPU as well.  The batched workload splits the instances over the ranks
+with no collective in the timed region (strong scaling).
 """
 from __future__ import annotations
 
@@ -366,6 +370,99 @@ def run_single(args, rank, world, local, torch, dist, _native):
     return line
 
 
+def run_sharded(args, rank, world, local, torch, dist, _native):
+    """One colony split over the ranks: m ants per rank, one packet
+    all-gather per epoch (NCCL) inside the timed region."""
+    from vehicleroutingproblem_b200 import sharding as S
+    wl = WORKLOADS[args.workload]
+    inst = wl["factory"]()
+    n, K, m, k = inst.n, inst.vehicles, wl["ants"], wl["cand_k"]
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    col = S.ShardedColony(inst, m, local, stream=stream, cand_k=k, seed=1234)
+    col.enqueue_epochs(args.warmup)
+    torch.cuda.synchronize()
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    steps0 = col.state().total_steps
+    dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        wall0 = time.perf_counter()
+        dev_ms = timed_steps(torch, stream, args.steps, col.enqueue_epoch, flush)
+        wall = time.perf_counter() - wall0
+    dist.barrier()
+    st = col.state()
+    assert st.error == 0 and st.epochs == args.warmup + args.steps
+    steps_all = float(st.total_steps - steps0)  # every rank's ants (packets carry them)
+    t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev_ms_max = float(t[0])
+    value = steps_all / (dev_ms_max / 1e3)
+    # Per-kernel times of this rank's epoch (plain path, local ants, after
+    # the timed region).
+    kms = col.ctx.profile_epochs(32) / 32.0
+    col.close()
+
+    e2e_vals = []
+    h2d = (n + 1) * (8 + 4) + 4095 * 4 + 2 * 256 * 4
+    d2h = (n + 2 * K) * 4 + K * 4
+    for i in range(args.e2e_steps):
+        dist.barrier()
+        t0 = time.perf_counter()
+        c2 = S.ShardedColony(inst, m, local, cand_k=k, seed=99 + i,
+                             fixed_epochs=wl["e2e_epochs"])
+        s2 = c2.run(wl["e2e_epochs"])
+        c2.best()
+        dt = time.perf_counter() - t0
+        c2.close()
+        td = torch.tensor([dt], dtype=torch.float64, device="cuda")
+        dist.all_reduce(td, op=dist.ReduceOp.MAX)
+        if i > 0:
+            e2e_vals.append(s2.total_steps / float(td[0]))
+    e2e = statistics.median(e2e_vals) if e2e_vals else None
+
+    peak, peak_kind = load_peaks()
+    bytes_per_step = k * (4 + 4 + 1)
+    local_steps_per_epoch = steps_all / args.steps / world
+    achieved = bytes_per_step * local_steps_per_epoch / (float(kms[1]) / 1e3) / 1e9
+    if rank != 0:
+        return None
+    packet_bytes = 4 * S.packet_ints(n, K)
+    line = {
+        "metric": "ant-steps/s", "value": value, "unit": "ant-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32 weights + u8 pheromone (f64 route costs)",
+        "data": "synthetic",
+        "config": {"workload": wl["name"], "n": n, "K": K, "capacity": inst.capacity,
+                   "ants": m * world, "ants_per_gpu": m, "cand_k": k, "step": "one epoch",
+                   "l2": "flushed between timed steps (256 MiB write outside the events)",
+                   "parallelism": f"one colony split over {world} GPU(s), packet all-gather "
+                                  f"({packet_bytes} B per rank) per epoch"},
+        "wall_s": wall,
+        "gpu_launches": 5 * args.steps,
+        "kernels_us": {"weights": float(kms[0]) * 1e3, "construct": float(kms[1]) * 1e3,
+                       "best": float(kms[2]) * 1e3, "evap_deposit": float(kms[3]) * 1e3},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak,
+                     "traffic": CONSTRUCT_DRAM_BYTES_PER_LAUNCH.get(args.workload),
+                     "kernel": "k_construct", "peak_kind": peak_kind,
+                     "bytes_per_ant_step": bytes_per_step},
+        "e2e": {"value": e2e, "unit": "ant-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "step": f"one split-colony solve: upload, candidates, {wl['e2e_epochs']} "
+                        "epochs with packet exchange, download of the best routes"},
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(inst, m, cand_k=k)
+        except Exception as exc:  # reported, not fatal
+            line["cpu_baseline"] = {"error": str(exc)[:200]}
+    return line
+
+
 def run_batched(args, rank, world, local, torch, dist, _native):
     insts_all = I.batched_instances(BATCHED["count"], BATCHED["seed0"])
     mine = list(range(rank, len(insts_all), world))  # this rank's slice
@@ -493,6 +590,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--looped-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--colony", default="auto", choices=["auto", "sharded"],
+                    help="single-instance workloads: auto = one GPU runs the plain "
+                         "graph-launched epochs, several GPUs split the colony")
     args = ap.parse_args()
     batched = args.workload == "batched"
     if args.steps is None:
@@ -514,15 +614,26 @@ def main():
     from vehicleroutingproblem_b200 import _native
 
     torch.cuda.set_device(local)
+    sharded = not batched and (world > 1 or args.colony == "sharded")
+    pg = world > 1 or sharded
     if world > 1:
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    elif pg:
+        import socket
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0,
+                                world_size=1, timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
     try:
-        fn = run_batched if batched else run_single
+        fn = run_batched if batched else (run_sharded if sharded else run_single)
         line = fn(args, rank, world, local, torch, dist, _native)
         if line is not None:
             print(json.dumps(line), flush=True)
     finally:
-        if world > 1:
+        if pg:
             dist.destroy_process_group()
     return 0
 

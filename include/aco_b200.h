@@ -57,6 +57,8 @@ typedef struct {
   int fixed_epochs;           /* 0 = no epoch limit                        */
   double min_rel_improvement; /* fraction (the env variable is percent)    */
   double timeout_seconds;     /* 0 = none                                  */
+  int ant_base;               /* global id of ant 0 (colony split over
+                                 devices); 0 for a whole colony            */
 } aco_b200_problem;
 
 /* Device-side solver state after a run. */
@@ -138,6 +140,29 @@ ACO_API int aco_b200_get_ants(aco_b200_ctx *ctx, int *nodes /* m (n+2K) */,
 ACO_API int aco_b200_evaporate_deposit(aco_b200_ctx *ctx, int best_ant,
                                float dep_iter, const int *gbest_nodes,
                                const int *gbest_lens, float dep_global);
+
+/*
+ * One colony split over several devices (one context per device, same
+ * instance and parameters, ants m each, ant_base = rank * m).  The pheromone
+ * matrix is replicated; per epoch each device
+ *   1. aco_b200_shard_construct: weights, construction of its m ants (random
+ *      draws keyed by the global ant id) and a packet with its best ant
+ *      (aco_b200_shard_packet_ints int32 words) written to d_send;
+ *   2. the caller all-gathers the packets of all devices (rank order) into
+ *      d_recv (e.g. ncclAllGather on the context stream);
+ *   3. aco_b200_shard_update: the winner over the packets (lowest cost, then
+ *      lowest global ant), the epoch bookkeeping and stop rules, evaporation
+ *      and the deposits, identical on every device.
+ * N devices with m ants each then run exactly the epochs of one device with
+ * N m ants.  Calls only enqueue work on the context stream.  The device
+ * timeout rule reads each device's own clock, so split colonies leave
+ * timeout_seconds at 0 and stop on the host.  Packet layout: [0,1] cost
+ * (FP64 bits), [2] found, [3] global ant, [4,5] ant-steps (64-bit), then K
+ * lengths and the compact route.
+ */
+ACO_API int aco_b200_shard_packet_ints(aco_b200_ctx *ctx);
+ACO_API int aco_b200_shard_construct(aco_b200_ctx *ctx, int32_t *d_send);
+ACO_API int aco_b200_shard_update(aco_b200_ctx *ctx, const int32_t *d_recv, int world);
 
 /*
  * Batched solving: many independent instances in one persistent launch.

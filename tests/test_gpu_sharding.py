@@ -1,0 +1,144 @@
+"""A colony split over devices (aco_b200_shard_*) equals one colony with all
+the ants.  One GPU stands in for the devices: two contexts with ant_base 0
+and m exchange their packets through a device buffer, epoch by epoch, and
+must follow one context with 2m ants exactly (pheromone, state, best)."""
+import numpy as np
+import pytest
+
+from vehicleroutingproblem_b200 import instances as I
+from vehicleroutingproblem_b200 import sharding as S
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "u150_unit": (lambda: I.uniform_instance(150, 4, 771, demand_max=1), 24, 16),
+    "u300_demand": (lambda: I.uniform_instance(300, 6, 772), 32, 24),
+    "c500_demand": (lambda: I.clustered_instance(500, 9, 773), 20, 32),
+}
+
+
+def _setup(N, inst, k, m, ant_base, stream, seed=99, **kw):
+    ctx = N.Context(0)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.setup_instance(inst, ants=m, cand_k=k, seed=seed, ant_base=ant_base, **kw)
+    return ctx
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_two_shards_equal_one_colony(native, name):
+    import torch
+    make, k, m = CASES[name]
+    inst = make()
+    n, K = inst.n, inst.vehicles
+    s = torch.cuda.Stream()
+    whole = _setup(native, inst, k, 2 * m, 0, s)
+    parts = [_setup(native, inst, k, m, r * m, s) for r in range(2)]
+    P = parts[0].shard_packet_ints()
+    assert P == S.packet_ints(n, K)
+    send = [torch.zeros(P, dtype=torch.int32, device="cuda") for _ in parts]
+    recv = torch.zeros(2 * P, dtype=torch.int32, device="cuda")
+    ranks_won = set()
+    for e in range(10):
+        for c, b in zip(parts, send):
+            c.shard_construct(b.data_ptr())
+        with torch.cuda.stream(s):
+            recv[:P].copy_(send[0])
+            recv[P:].copy_(send[1])
+        for c in parts:
+            c.shard_update(recv.data_ptr(), 2)
+        whole.enqueue_epochs(1)
+        s.synchronize()
+        # the packets hold each half's best ant, with the ant-steps
+        nodes, lens, cost, feas, steps, _ = whole.ants()
+        pk = [S.decode_packet(recv[r * P:(r + 1) * P].cpu().numpy(), n, K) for r in range(2)]
+        for r in range(2):
+            sl = slice(r * m, (r + 1) * m)
+            c = np.where(feas[sl] != 0, cost[sl], np.inf)
+            assert pk[r].steps == int(steps[sl].sum())
+            assert pk[r].found == bool(np.isfinite(c).any())
+            if pk[r].found:
+                b = int(np.argmin(c))
+                assert pk[r].global_ant == r * m + b and pk[r].cost == c[b]
+                assert np.array_equal(pk[r].lens, lens[r * m + b])
+                assert np.array_equal(pk[r].nodes, nodes[r * m + b][: int(lens[r * m + b].sum())])
+        sw = whole.state()
+        wi = S.select_winner(pk)
+        if wi is not None:
+            ranks_won.add(wi)
+            assert sw.best_ant == pk[wi].global_ant
+        t = whole.tau()
+        for c in parts:
+            st = c.state()
+            assert (st.epochs, st.found, st.best_ant, st.iter_since_best, st.improved) == \
+                (sw.epochs, sw.found, sw.best_ant, sw.iter_since_best, sw.improved)
+            assert st.global_best == sw.global_best and st.iter_best == sw.iter_best
+            assert st.dep_iter == sw.dep_iter and st.dep_global == sw.dep_global
+            assert st.total_steps == sw.total_steps and st.error == 0
+            assert np.array_equal(c.tau(), t)
+            bn, bl, bc = c.best()
+            wn, wl, wc = whole.best()
+            assert bc == wc and np.array_equal(bl, wl) and np.array_equal(bn, wn)
+    assert ranks_won == {0, 1}
+    for c in parts + [whole]:
+        c.close()
+
+
+def test_stop_rules_agree_across_shards(native):
+    """Stagnation stops every shard after the same epoch as the whole colony;
+    the epochs queued after it are skipped."""
+    import torch
+    inst = I.uniform_instance(120, 3, 774)
+    s = torch.cuda.Stream()
+    whole = _setup(native, inst, 16, 32, 0, s, stagnation_epochs=3)
+    st_w = whole.run(400)
+    assert st_w.stopped and st_w.epochs < 400
+    parts = [_setup(native, inst, 16, 16, r * 16, s, stagnation_epochs=3) for r in range(2)]
+    P = parts[0].shard_packet_ints()
+    send = [torch.zeros(P, dtype=torch.int32, device="cuda") for _ in parts]
+    recv = torch.zeros(2 * P, dtype=torch.int32, device="cuda")
+    for e in range(st_w.epochs + 5):
+        for c, b in zip(parts, send):
+            c.shard_construct(b.data_ptr())
+        with torch.cuda.stream(s):
+            recv[:P].copy_(send[0])
+            recv[P:].copy_(send[1])
+        for c in parts:
+            c.shard_update(recv.data_ptr(), 2)
+    s.synchronize()
+    for c in parts:
+        st = c.state()
+        assert st.stopped and st.epochs == st_w.epochs
+        assert st.global_best == st_w.global_best
+        assert np.array_equal(c.tau(), whole.tau())
+        c.close()
+    whole.close()
+
+
+def test_sharded_colony_over_nccl_world_one(native):
+    """ShardedColony through a real NCCL process group (one rank) follows the
+    plain context epoch for epoch."""
+    import os
+    import socket
+    import torch
+    import torch.distributed as dist
+    inst = I.uniform_instance(200, 5, 775)
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0))
+    try:
+        col = S.ShardedColony(inst, 48, 0, cand_k=16, seed=5)
+        st = col.run(37, chunk=16)
+        ref = _setup(native, inst, 16, 48, 0, torch.cuda.Stream(), seed=5)
+        st_r = ref.run(37)
+        assert st.epochs == st_r.epochs == 37
+        assert st.global_best == st_r.global_best and st.total_steps == st_r.total_steps
+        assert np.array_equal(col.tau(), ref.tau())
+        pk = col.packets()
+        assert len(pk) == 1 and pk[0].found and pk[0].global_ant == st_r.best_ant
+        col.close()
+        ref.close()
+    finally:
+        dist.destroy_process_group()

@@ -38,6 +38,7 @@ EXPORTED = [
     "aco_b200_batch_set_tuning", "aco_b200_batch_get_tuning", "aco_b200_batch_autotune",
     "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
     "aco_b200_batch_get", "aco_b200_batch_get_costs",
+    "aco_b200_shard_packet_ints", "aco_b200_shard_construct", "aco_b200_shard_update",
     "aco_status_string", "aco_vrp_cuda_with_capacity", "aco_vrp_cuda_with_demands",
     "solution_create", "solution_free", "solution_reset", "solution_copy",
     "solution_cost", "route_append", "solution_validate",
@@ -64,7 +65,8 @@ class Problem(C.Structure):
                 ("alpha", C.c_double), ("beta", C.c_double), ("rho", C.c_double),
                 ("tau0", C.c_double), ("Q", C.c_double), ("seed", C.c_uint),
                 ("stagnation_epochs", C.c_int), ("fixed_epochs", C.c_int),
-                ("min_rel_improvement", C.c_double), ("timeout_seconds", C.c_double)]
+                ("min_rel_improvement", C.c_double), ("timeout_seconds", C.c_double),
+                ("ant_base", C.c_int)]
 
 
 class State(C.Structure):
@@ -126,6 +128,8 @@ def load():
         "aco_b200_batch_synchronize": [vp],
         "aco_b200_batch_get": [vp, i32, vp, vp, vp, vp],
         "aco_b200_batch_get_costs": [vp, vp, vp, vp],
+        "aco_b200_shard_packet_ints": [vp], "aco_b200_shard_construct": [vp, vp],
+        "aco_b200_shard_update": [vp, vp, i32],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)
@@ -181,7 +185,8 @@ class Context:
     def setup(self, x, y, K: int, capacity: int, demand=None, ants: int = 256,
               cand_k: int = 0, alpha=1.0, beta=2.0, rho=0.5, tau0=1.0, Q=1.0,
               seed: int = 1234, stagnation_epochs: int = 0, fixed_epochs: int = 0,
-              min_rel_improvement: float = 1e-3, timeout_seconds: float = 0.0):
+              min_rel_improvement: float = 1e-3, timeout_seconds: float = 0.0,
+              ant_base: int = 0):
         x = np.ascontiguousarray(x, np.float32)
         y = np.ascontiguousarray(y, np.float32)
         d = None if demand is None else np.ascontiguousarray(demand, np.int32)
@@ -190,7 +195,8 @@ class Context:
                     x=_p(x).value, y=_p(y).value, demand=None if d is None else _p(d).value,
                     alpha=alpha, beta=beta, rho=rho, tau0=tau0, Q=Q, seed=seed & 0xffffffff,
                     stagnation_epochs=stagnation_epochs, fixed_epochs=fixed_epochs,
-                    min_rel_improvement=min_rel_improvement, timeout_seconds=timeout_seconds)
+                    min_rel_improvement=min_rel_improvement, timeout_seconds=timeout_seconds,
+                    ant_base=ant_base)
         _check(self._lib.aco_b200_setup(self._h, C.byref(p)), "aco_b200_setup")
         n, K_, k, m = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         _check(self._lib.aco_b200_get_dims(self._h, C.byref(n), C.byref(K_), C.byref(k),
@@ -296,6 +302,26 @@ class Context:
         _check(self._lib.aco_b200_evaporate_deposit(self._h, best_ant, dep_iter, _p(gn),
                                                     _p(gl), dep_global),
                "aco_b200_evaporate_deposit")
+
+    # --- colony split over several devices (aco_b200_shard_*) -------------
+
+    def shard_packet_ints(self) -> int:
+        P = self._lib.aco_b200_shard_packet_ints(self._h)
+        if P < 0:
+            raise AcoError(ACO_ERR_INVALID_INPUT, "aco_b200_shard_packet_ints")
+        return P
+
+    def shard_construct(self, d_send: int) -> None:
+        """Enqueues weights, construction and the packet of this device's best
+        ant into the device buffer at address d_send."""
+        _check(self._lib.aco_b200_shard_construct(self._h, C.c_void_p(d_send)),
+               "aco_b200_shard_construct")
+
+    def shard_update(self, d_recv: int, world: int) -> None:
+        """Enqueues winner selection over `world` gathered packets at device
+        address d_recv, bookkeeping, evaporation and deposits."""
+        _check(self._lib.aco_b200_shard_update(self._h, C.c_void_p(d_recv), world),
+               "aco_b200_shard_update")
 
 
 class BatchProblem(C.Structure):

@@ -98,6 +98,7 @@ struct InstanceView {
   int unit;                // 1: every customer has demand 1
   int max_demand;          // largest customer demand
   int route_stride;        // n + 2K
+  int ant_base;            // global id of local ant 0 (colony split over devices)
   const float2 *coords;    // [n+1]
   const int *demand;       // [n+1]
   const uint16_t *cand;    // [(n+1) k]
@@ -154,6 +155,18 @@ cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
                                 unsigned int *counter, int grid,
                                 cudaStream_t s);
 cudaError_t launch_set_run_limit(DevState *st, int limit, cudaStream_t s);
+int shard_packet_size(int n, int K);
+cudaError_t launch_shard_pack(const InstanceView &iv, const AntBuffers &ab, DevState *st,
+                              int *send, cudaStream_t s);
+cudaError_t launch_shard_select(const InstanceView &iv, DevState *st, const int *recv,
+                                int world, int *iter_nodes, int *iter_lens,
+                                int *gbest_nodes, int *gbest_lens, EpochRec *log,
+                                cudaStream_t s);
+cudaError_t launch_evap_deposit_iter(const InstanceView &iv, const PheromoneView &pv,
+                                     const AntBuffers &ab, DevState *st,
+                                     const int *iter_nodes, const int *iter_lens,
+                                     const int *gbest_nodes, const int *gbest_lens,
+                                     unsigned int *counter, int grid, cudaStream_t s);
 int construct_max_smem();
 cudaError_t prepare_construct_kernels();
 SmemPlan plan_construct(const InstanceView &iv, int layout, int num_sms,

@@ -330,8 +330,11 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
   int *lens = a.ab.lens + (size_t)ant * K;
   int *loads = a.ab.loads + (size_t)ant * K;
 
+  // Draws are keyed by the ant's global id (ant_base > 0 when the colony is
+  // split over several devices).
+  const uint32_t gant = (uint32_t)(ant + iv.ant_base);
   uint32_t d = 0;
-  draw_refill(dbuf, d, a.seed, epoch, (uint32_t)ant, a.stream, lane);
+  draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
   uint32_t r_next = dbuf[0];
 
   int remaining = iv.n;
@@ -415,7 +418,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       // A draw is consumed only by a roulette selection (denom > 0).
       d += (denom != 0u) ? 1u : 0u;
       if ((d & 127u) == 0u && denom != 0u)
-        draw_refill(dbuf, d, a.seed, epoch, (uint32_t)ant, a.stream, lane);
+        draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
       r_next = dbuf[d & 127u];
     }
     if (lane == 0) {
@@ -701,6 +704,53 @@ __device__ __forceinline__ bool significant(double prev, double next,
   return __dadd_rn(rel, 1e-9) >= min_rel;
 }
 
+// Epoch bookkeeping of src/cuda/aco_cuda.cu:349-399 and the stop rules
+// checked at the start of the next epoch (:333-339), given the iteration's
+// best feasible ant (found, cost bc, ant ba) and its ant-steps.  Returns
+// whether the global best improved.
+__device__ int epoch_bookkeeping(DevState *st, bool found, double bc, int ba,
+                                 unsigned long long steps, EpochRec *log) {
+  int improved = 0;
+  st->found = found ? 1 : 0;
+  st->total_steps += steps;
+  if (found) {
+    st->iter_best = bc;
+    st->best_ant = ba;
+    if (bc < st->global_best) {
+      improved = 1;
+      if (significant(st->global_best, bc, st->min_rel)) st->iter_since_best = 0;
+      else st->iter_since_best += 1;
+      st->global_best = bc;
+    } else {
+      st->iter_since_best += 1;
+    }
+    st->dep_iter = __fdiv_rn(0.3f * st->Qs, (float)bc);
+    st->dep_global = __fdiv_rn(0.7f * st->Qs, (float)st->global_best);
+  } else {
+    st->iter_since_best += 1;
+  }
+  st->improved = improved;
+  st->epoch += 1;
+  const unsigned long long now = global_timer_ns();
+  const unsigned long long elapsed = now > st->start_ns ? now - st->start_ns : 0ull;
+  EpochRec rec;
+  rec.epoch = st->epoch;
+  rec.iter_since_best = st->iter_since_best;
+  rec.improved = improved;
+  rec.found = found ? 1 : 0;
+  rec.global_best = st->global_best;
+  rec.elapsed_ns = elapsed;
+  log[st->log_count % kLogCap] = rec;
+  st->log_count += 1;
+  int flags = st->stop_flags;
+  if (st->stagnation > 0 && st->iter_since_best >= st->stagnation) flags |= kStopStagnation;
+  if (st->fixed_epochs > 0 && st->epoch >= st->fixed_epochs) flags |= kStopFixed;
+  if (st->timeout_ns > 0ull && elapsed > st->timeout_ns) flags |= kStopTimeout;
+  if (st->run_limit > 0 && st->epoch >= st->run_limit) flags |= kStopRunLimit;
+  st->stop_flags = flags;
+  return improved;
+}
+
 __global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
                                                DevState *st, int *gbest_nodes,
                                                int *gbest_lens, EpochRec *log) {
@@ -755,47 +805,7 @@ __global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
       }
     }
     if (lane == 0) {
-      // Epoch bookkeeping of src/cuda/aco_cuda.cu:349-399 and the stop
-      // rules checked at the start of the next epoch (:333-339).
-      const bool found = (ba != INT_MAX);
-      int improved = 0;
-      st->found = found ? 1 : 0;
-      st->total_steps += steps;
-      if (found) {
-        st->iter_best = bc;
-        st->best_ant = ba;
-        if (bc < st->global_best) {
-          improved = 1;
-          if (significant(st->global_best, bc, st->min_rel)) st->iter_since_best = 0;
-          else st->iter_since_best += 1;
-          st->global_best = bc;
-        } else {
-          st->iter_since_best += 1;
-        }
-        st->dep_iter = __fdiv_rn(0.3f * st->Qs, (float)bc);
-        st->dep_global = __fdiv_rn(0.7f * st->Qs, (float)st->global_best);
-      } else {
-        st->iter_since_best += 1;
-      }
-      st->improved = improved;
-      st->epoch += 1;
-      const unsigned long long now = global_timer_ns();
-      const unsigned long long elapsed = now > st->start_ns ? now - st->start_ns : 0ull;
-      EpochRec rec;
-      rec.epoch = st->epoch;
-      rec.iter_since_best = st->iter_since_best;
-      rec.improved = improved;
-      rec.found = found ? 1 : 0;
-      rec.global_best = st->global_best;
-      rec.elapsed_ns = elapsed;
-      log[st->log_count % kLogCap] = rec;
-      st->log_count += 1;
-      int flags = st->stop_flags;
-      if (st->stagnation > 0 && st->iter_since_best >= st->stagnation) flags |= kStopStagnation;
-      if (st->fixed_epochs > 0 && st->epoch >= st->fixed_epochs) flags |= kStopFixed;
-      if (st->timeout_ns > 0ull && elapsed > st->timeout_ns) flags |= kStopTimeout;
-      if (st->run_limit > 0 && st->epoch >= st->run_limit) flags |= kStopRunLimit;
-      st->stop_flags = flags;
+      const int improved = epoch_bookkeeping(st, ba != INT_MAX, bc, ba, steps, log);
       s_improved = improved;
       s_best = ba;
     }
@@ -847,6 +857,8 @@ struct EvapArgs {
   DevState *st;
   const int *gbest_nodes;
   const int *gbest_lens;
+  const int *iter_nodes;  // iteration best from an exchange (else best ant's)
+  const int *iter_lens;
   unsigned int *counter;
   int best_ant;          // used when st == nullptr
   float dep_iter, dep_global;
@@ -902,8 +914,11 @@ __global__ void __launch_bounds__(512) k_evap_deposit(EvapArgs a) {
   const float dep_g = a.st ? a.st->dep_global : a.dep_global;
   extern __shared__ int s_off[];
   int *offs = (a.iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
-  deposit_solution(pv, stride_n, CompactNodes{a.ab.routes + (size_t)best * a.iv.route_stride},
-                   a.ab.lens + (size_t)best * a.iv.K, a.iv.K, dep_i, offs);
+  if (a.iter_nodes)
+    deposit_solution(pv, stride_n, CompactNodes{a.iter_nodes}, a.iter_lens, a.iv.K, dep_i, offs);
+  else
+    deposit_solution(pv, stride_n, CompactNodes{a.ab.routes + (size_t)best * a.iv.route_stride},
+                     a.ab.lens + (size_t)best * a.iv.K, a.iv.K, dep_i, offs);
   __syncthreads();
   if (a.gbest_nodes) {
     deposit_solution(pv, stride_n, CompactNodes{a.gbest_nodes}, a.gbest_lens, a.iv.K, dep_g, offs);
@@ -923,6 +938,8 @@ cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
   a.st = st;
   a.gbest_nodes = gbest_nodes;
   a.gbest_lens = gbest_lens;
+  a.iter_nodes = nullptr;
+  a.iter_lens = nullptr;
   a.counter = counter;
   a.best_ant = 0;
   a.dep_iter = a.dep_global = 0.0f;
@@ -948,10 +965,180 @@ cudaError_t launch_evap_deposit_explicit(const InstanceView &iv,
   a.st = nullptr;
   a.gbest_nodes = gbest_nodes;
   a.gbest_lens = gbest_lens;
+  a.iter_nodes = nullptr;
+  a.iter_lens = nullptr;
   a.counter = counter;
   a.best_ant = best_ant;
   a.dep_iter = dep_iter;
   a.dep_global = dep_global;
+  const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
+  k_evap_deposit<<<grid, 512, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+// ===========================================================================
+// Colony split over several devices: local best packet, exchange, winner
+// ===========================================================================
+
+// Packet of one device's iteration best (int32 words):
+//   [0,1] cost (FP64 bits; DBL_MAX when no feasible ant)  [2] found
+//   [3] global ant id  [4,5] ant-steps of all local ants  [6, 6+K) lengths
+//   [6+K, 6+K+n+2K) compact route.
+__host__ __device__ inline int shard_packet_ints(int n, int K) {
+  return (6 + K + n + 2 * K + 3) & ~3;
+}
+
+__global__ void __launch_bounds__(1024) k_shard_pack(InstanceView iv, AntBuffers ab,
+                                                     DevState *st, int *send) {
+  __shared__ double s_cost[32];
+  __shared__ int s_ant[32];
+  __shared__ unsigned long long s_steps[32];
+  __shared__ int s_best;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool skip = *(volatile int *)&st->skip;
+  double bc = DBL_MAX;
+  int ba = INT_MAX;
+  unsigned long long steps = 0;
+  for (int i = threadIdx.x; i < iv.m && !skip; i += blockDim.x) {
+    steps += (unsigned long long)ab.steps[i];
+    if (ab.feasible[i]) {
+      const double c = ab.cost[i];
+      if (ba == INT_MAX || c < bc) {
+        bc = c;
+        ba = i;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double oc = __shfl_down_sync(kFull, bc, o);
+    const int oa = __shfl_down_sync(kFull, ba, o);
+    steps += __shfl_down_sync(kFull, steps, o);
+    if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
+      bc = oc;
+      ba = oa;
+    }
+  }
+  if (lane == 0) {
+    s_cost[warp] = bc;
+    s_ant[warp] = ba;
+    s_steps[warp] = steps;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bc = DBL_MAX;
+    ba = INT_MAX;
+    steps = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      steps += s_steps[w];
+      const double oc = s_cost[w];
+      const int oa = s_ant[w];
+      if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
+        bc = oc;
+        ba = oa;
+      }
+    }
+    const unsigned long long cb = (unsigned long long)__double_as_longlong(bc);
+    send[0] = (int)(cb & 0xffffffffu);
+    send[1] = (int)(cb >> 32);
+    send[2] = (ba != INT_MAX) ? 1 : 0;
+    send[3] = (ba != INT_MAX) ? ba + iv.ant_base : INT_MAX;
+    send[4] = (int)(steps & 0xffffffffu);
+    send[5] = (int)(steps >> 32);
+    s_best = ba;
+  }
+  __syncthreads();
+  if (s_best != INT_MAX) {
+    const int *src = ab.routes + (size_t)s_best * iv.route_stride;
+    const int *sl = ab.lens + (size_t)s_best * iv.K;
+    for (int v = threadIdx.x; v < iv.K; v += blockDim.x) send[6 + v] = sl[v];
+    int total = 0;
+    for (int v = 0; v < iv.K; ++v) total += sl[v];
+    for (int t = threadIdx.x; t < total; t += blockDim.x) send[6 + iv.K + t] = src[t];
+  }
+}
+
+// Winner over the gathered packets (lowest cost, then lowest global ant:
+// the first minimum a single device holding every ant would find), then the
+// same bookkeeping as k_best; its route goes to iter_nodes/iter_lens and,
+// on improvement, to the global best.
+__global__ void __launch_bounds__(256) k_shard_select(InstanceView iv, DevState *st,
+                                                      const int *recv, int world,
+                                                      int *iter_nodes, int *iter_lens,
+                                                      int *gbest_nodes, int *gbest_lens,
+                                                      EpochRec *log) {
+  if (*(volatile int *)&st->skip) return;
+  __shared__ int s_src, s_improved;
+  const int P = shard_packet_ints(iv.n, iv.K);
+  if (threadIdx.x == 0) {
+    double bc = DBL_MAX;
+    int ba = INT_MAX, src = -1;
+    unsigned long long steps = 0;
+    for (int r = 0; r < world; ++r) {
+      const int *pk = recv + (size_t)r * P;
+      steps += (unsigned long long)(unsigned)pk[4] | ((unsigned long long)(unsigned)pk[5] << 32);
+      if (!pk[2]) continue;
+      const double c = __longlong_as_double(
+          (long long)((unsigned long long)(unsigned)pk[0] | ((unsigned long long)(unsigned)pk[1] << 32)));
+      const int ga = pk[3];
+      if (src < 0 || c < bc || (c == bc && ga < ba)) {
+        bc = c;
+        ba = ga;
+        src = r;
+      }
+    }
+    s_improved = epoch_bookkeeping(st, src >= 0, bc, ba, steps, log);
+    s_src = src;
+  }
+  __syncthreads();
+  if (s_src < 0) return;
+  const int *pk = recv + (size_t)s_src * P;
+  int total = 0;
+  for (int v = 0; v < iv.K; ++v) total += pk[6 + v];
+  for (int v = threadIdx.x; v < iv.K; v += blockDim.x) {
+    iter_lens[v] = pk[6 + v];
+    if (s_improved) gbest_lens[v] = pk[6 + v];
+  }
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    iter_nodes[t] = pk[6 + iv.K + t];
+    if (s_improved) gbest_nodes[t] = pk[6 + iv.K + t];
+  }
+}
+
+int shard_packet_size(int n, int K) { return shard_packet_ints(n, K); }
+
+cudaError_t launch_shard_pack(const InstanceView &iv, const AntBuffers &ab, DevState *st,
+                              int *send, cudaStream_t s) {
+  k_shard_pack<<<1, 1024, 0, s>>>(iv, ab, st, send);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_shard_select(const InstanceView &iv, DevState *st, const int *recv,
+                                int world, int *iter_nodes, int *iter_lens,
+                                int *gbest_nodes, int *gbest_lens, EpochRec *log,
+                                cudaStream_t s) {
+  k_shard_select<<<1, 256, 0, s>>>(iv, st, recv, world, iter_nodes, iter_lens, gbest_nodes,
+                                   gbest_lens, log);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_evap_deposit_iter(const InstanceView &iv, const PheromoneView &pv,
+                                     const AntBuffers &ab, DevState *st,
+                                     const int *iter_nodes, const int *iter_lens,
+                                     const int *gbest_nodes, const int *gbest_lens,
+                                     unsigned int *counter, int grid, cudaStream_t s) {
+  EvapArgs a;
+  a.iv = iv;
+  a.pv = pv;
+  a.ab = ab;
+  a.st = st;
+  a.gbest_nodes = gbest_nodes;
+  a.gbest_lens = gbest_lens;
+  a.iter_nodes = iter_nodes;
+  a.iter_lens = iter_lens;
+  a.counter = counter;
+  a.best_ant = 0;
+  a.dep_iter = a.dep_global = 0.0f;
   const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
   k_evap_deposit<<<grid, 512, smem, s>>>(a);
   return cudaGetLastError();

@@ -84,6 +84,7 @@ struct aco_b200_ctx {
   EpochRec *d_log = nullptr;
   int *d_gbest_nodes = nullptr, *d_gbest_lens = nullptr;
   int *d_tmp_nodes = nullptr, *d_tmp_lens = nullptr;
+  int *d_iter_nodes = nullptr, *d_iter_lens = nullptr;  // exchanged iteration best
   unsigned int *d_counter = nullptr;
 
   // host mirrors
@@ -111,14 +112,16 @@ void aco_b200_ctx::free_buffers() {
   void *ptrs[] = {d_coords, d_demand, d_cand, d_lvl, d_thr, d_A, d_lut, d_tau,
                   d_w, d_rel, ab.routes, ab.lens, ab.cost, ab.feasible, ab.steps,
                   ab.draws, ab.loads, ab.rep, ab.repc, d_state, d_log,
-                  d_gbest_nodes, d_gbest_lens, d_tmp_nodes, d_tmp_lens, d_counter};
+                  d_gbest_nodes, d_gbest_lens, d_tmp_nodes, d_tmp_lens, d_iter_nodes,
+                  d_iter_lens, d_counter};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d_coords = nullptr; d_demand = nullptr; d_cand = d_lvl = nullptr; d_thr = nullptr;
   d_A = nullptr; d_lut = nullptr; d_tau = nullptr; d_w = nullptr; d_rel = nullptr;
   ab = AntBuffers{};
   d_state = nullptr; d_log = nullptr; d_gbest_nodes = d_gbest_lens = nullptr;
-  d_tmp_nodes = d_tmp_lens = nullptr; d_counter = nullptr;
+  d_tmp_nodes = d_tmp_lens = nullptr; d_iter_nodes = d_iter_lens = nullptr;
+  d_counter = nullptr;
   ready = false;
 }
 
@@ -312,6 +315,10 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   if (k > n) k = n;
   int m = p->ants > 0 ? p->ants : 256;
   if ((long long)m * (n + 2LL * p->K) > (1LL << 31)) return ACO_ERR_INVALID_INPUT;
+  if (p->ant_base < 0 || (long long)p->ant_base + m > 0x7fffffffLL) {
+    fprintf(stderr, "aco_b200: invalid ant_base=%d\n", p->ant_base);
+    return ACO_ERR_INVALID_INPUT;
+  }
 
   cudaSetDevice(ctx->device);
   ctx->free_buffers();
@@ -355,6 +362,8 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   TRY_ALLOC(dalloc(&ctx->d_gbest_lens, (size_t)p->K));
   TRY_ALLOC(dalloc(&ctx->d_tmp_nodes, (size_t)R));
   TRY_ALLOC(dalloc(&ctx->d_tmp_lens, (size_t)p->K));
+  TRY_ALLOC(dalloc(&ctx->d_iter_nodes, (size_t)R));
+  TRY_ALLOC(dalloc(&ctx->d_iter_lens, (size_t)p->K));
   TRY_ALLOC(dalloc(&ctx->d_counter, 1));
 
   std::vector<float2> xy(rows);
@@ -379,6 +388,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   iv.unit = unit ? 1 : 0;
   iv.max_demand = max_demand;
   iv.route_stride = R;
+  iv.ant_base = p->ant_base;
   iv.coords = ctx->d_coords;
   iv.demand = ctx->d_demand;
   iv.cand = ctx->d_cand;
@@ -517,6 +527,37 @@ int aco_b200_enqueue_epochs(aco_b200_ctx *ctx, int epochs) {
     left -= kChunkEpochs;
   }
   for (int i = 0; i < left; ++i) TRY(cudaGraphLaunch(ctx->graph_one, s));
+  return ACO_OK;
+}
+
+int aco_b200_shard_packet_ints(aco_b200_ctx *ctx) {
+  if (!ctx || !ctx->ready) return -1;
+  return shard_packet_size(ctx->n, ctx->K);
+}
+
+int aco_b200_shard_construct(aco_b200_ctx *ctx, int32_t *d_send) {
+  if (!ctx || !ctx->ready || !d_send) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if (!ctx->run_limit_off) {
+    TRY(launch_set_run_limit(ctx->d_state, 0, s));
+    ctx->run_limit_off = true;
+  }
+  TRY(launch_weights(ctx->iv, ctx->pv, ctx->et, ctx->d_state, s));
+  TRY(launch_construct(ctx->iv, ctx->et, ctx->ab, ctx->plan, ctx->d_state, ctx->seed, 0, 0, 1, s));
+  TRY(launch_shard_pack(ctx->iv, ctx->ab, ctx->d_state, d_send, s));
+  return ACO_OK;
+}
+
+int aco_b200_shard_update(aco_b200_ctx *ctx, const int32_t *d_recv, int world) {
+  if (!ctx || !ctx->ready || !d_recv || world < 1) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  TRY(launch_shard_select(ctx->iv, ctx->d_state, d_recv, world, ctx->d_iter_nodes,
+                          ctx->d_iter_lens, ctx->d_gbest_nodes, ctx->d_gbest_lens, ctx->d_log, s));
+  TRY(launch_evap_deposit_iter(ctx->iv, ctx->pv, ctx->ab, ctx->d_state, ctx->d_iter_nodes,
+                               ctx->d_iter_lens, ctx->d_gbest_nodes, ctx->d_gbest_lens,
+                               ctx->d_counter, ctx->evap_grid, s));
   return ACO_OK;
 }
 

@@ -22,6 +22,11 @@ solve of the whole batch and the metric is instances/s.
   on the host.
 * roofline: the dominant kernel, algorithmic bytes per ant-step k(4 + 4 + 1)
   (candidate id, weight, pheromone byte) over its mean event-timed duration.
+* cli_same_contract / reference_cuda_same_gpu (reference arm): this
+  library's aco_vrp_cuda.out and the reference's own CUDA solver (built from
+  its sources for sm_100a) run through the same CLI on the same GPU and the
+  unit-demand twin, epochs per second from their final progress line under
+  ACO_SOLVER_TIMEOUT_SECONDS.
 * cpu_baseline / --impl reference: the reference's OpenMP solver
   (oracle/_ref/aco_vrp_omp.out, built from the reference sources) on the
   unit-demand twins with all host threads and fixed epochs; the oracle port
@@ -72,6 +77,9 @@ BATCHED = dict(count=512, seed0=30000, ants=64, cand_k=16, epochs=300,
 # bytes.  Other workloads report null.
 CONSTRUCT_DRAM_BYTES_PER_LAUNCH = {"n1000": 234496}
 OMP_BIN = os.path.join(ROOT, "oracle", "_ref", "aco_vrp_omp.out")
+REF_CUDA_BIN = os.path.join(ROOT, "oracle", "_ref", "aco_vrp_cuda_ref.out")
+OUR_CLI = os.path.join(ROOT, "aco_vrp_cuda.out")
+CLI_SECONDS = 4.0
 
 
 def load_peaks():
@@ -229,6 +237,36 @@ def cpu_baseline_batched(insts, target_s=15.0):
                        f"to the batch by n+K, OMP_NUM_THREADS={threads}")}
 
 
+def cli_epoch_rate(binary, inst, ants, seconds=CLI_SECONDS):
+    """Epoch rate of a solver binary with the reference CLI contract
+    (`<vrp> <K> <m> <seed>`, ACO_SOLVER_* env) on the unit-demand twin, from
+    its last `[progress][cuda] epoca=E | ... tempo_trascorso=S s` line under
+    ACO_SOLVER_TIMEOUT_SECONDS (the timer starts after set-up)."""
+    import re
+    twin = inst.unit_twin()
+    n, K = twin.n, twin.vehicles
+    env = dict(os.environ, ACO_SOLVER_TIMEOUT_SECONDS=str(seconds),
+               ACO_SOLVER_STAGNATION_EPOCHS="0", ACO_SOLVER_PROGRESS_INTERVAL_SECONDS="0")
+    env.pop("ACO_SOLVER_FIXED_EPOCHS", None)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, twin.name + ".vrp")
+        I.write_vrp(twin, path)
+        r = subprocess.run([binary, path, str(K), str(ants), "1234"], env=env,
+                           capture_output=True, text=True, timeout=seconds + 300)
+    if r.returncode != 0:
+        return {"error": f"exit {r.returncode}: {r.stderr[-300:]}"}
+    prog = re.findall(r"epoca=(\d+) .*tempo_trascorso=([0-9.]+)s", r.stdout)
+    cost = re.findall(r"best cost: ([0-9.]+)", r.stdout)
+    if not prog:
+        return {"error": "no progress line"}
+    e, sec = int(prog[-1][0]), float(prog[-1][1])
+    return {"epochs": e, "seconds": sec, "epochs_per_s": e / sec,
+            "ant_steps_per_s_max": ants * (n + K) * e / sec,
+            "best_cost": float(cost[-1]) if cost else None,
+            "instance": f"unit-demand twin n={n} K={K} capacity={twin.capacity}",
+            "ants": ants, "timeout_s": seconds}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -246,12 +284,22 @@ def run_reference_arm(args, rank, world):
                "cand_k": wl["cand_k"]}
         metric, unit = "ant-steps/s", "ant-steps/s"
     cfg["note"] = "reference CPU path runs the unit-demand twins (its parser accepts demand 1 only)"
+    ref_gpu = None
+    if args.workload != "batched" and os.path.exists(REF_CUDA_BIN):
+        # The reference's own CUDA solver (built from its sources for sm_100a)
+        # on this machine's GPU, same CLI contract: the GPU bar to beat.
+        try:
+            ref_gpu = cli_epoch_rate(REF_CUDA_BIN, inst, wl["ants"])
+        except Exception as exc:  # reported, not fatal
+            ref_gpu = {"error": str(exc)[:200]}
     line = {"impl": "reference", "metric": metric, "value": cb.get("value"), "unit": unit,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "data": "synthetic", "config": cfg, "cpu_baseline": cb,
             "e2e": {"value": cb.get("value"), "unit": unit, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    if ref_gpu is not None:
+        line["reference_cuda_same_gpu"] = ref_gpu
     print(json.dumps(line), flush=True)
     return 0
 
@@ -366,6 +414,13 @@ def run_single(args, rank, world, local, torch, dist, _native):
                 line["cpu_baseline"] = cpu_baseline(inst, m, cand_k=k)
             except Exception as exc:  # reported, not fatal
                 line["cpu_baseline"] = {"error": str(exc)[:200]}
+        if world == 1 and args.cli and os.path.exists(OUR_CLI):
+            # This library's drop-in CLI under the reference's CLI contract,
+            # comparable with the reference arm's reference_cuda_same_gpu.
+            try:
+                line["cli_same_contract"] = cli_epoch_rate(OUR_CLI, inst, m)
+            except Exception as exc:  # reported, not fatal
+                line["cli_same_contract"] = {"error": str(exc)[:200]}
     ctx.close()
     return line
 
@@ -590,6 +645,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--looped-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cli", dest="cli", action="store_false",
+                    help="skip the drop-in CLI timing on the unit-demand twin")
     ap.add_argument("--colony", default="auto", choices=["auto", "sharded"],
                     help="single-instance workloads: auto = one GPU runs the plain "
                          "graph-launched epochs, several GPUs split the colony")

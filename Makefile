@@ -19,7 +19,7 @@ BUILD := $(PKG)/_build
 LIB := $(PKG)/libaco_b200.so
 CLI := aco_vrp_cuda.out
 
-CU_SRCS := $(CSRC)/cuda/aco_kernels.cu $(CSRC)/cuda/aco_solver.cu $(CSRC)/cuda/aco_compat.cu \
+CU_SRCS := $(CSRC)/cuda/aco_kernels.cu $(CSRC)/cuda/aco_solver.cu $(CSRC)/cuda/aco_compat.cu $(CSRC)/cuda/aco_prior.cu \
            $(CSRC)/cuda/aco_noalloc.cu $(CSRC)/cuda/aco_batch.cu
 C_SRCS := $(CSRC)/common/solution.c $(CSRC)/common/instance_parser.c \
           $(CSRC)/common/aco_config.c $(CSRC)/common/cli_common.c

@@ -165,6 +165,64 @@ ACO_API int aco_b200_shard_construct(aco_b200_ctx *ctx, int32_t *d_send);
 ACO_API int aco_b200_shard_update(aco_b200_ctx *ctx, const int32_t *d_recv, int world);
 
 /*
+ * Learned heuristic prior.  A small MLP (8 candidate-edge features -> 64 ->
+ * 64 -> 1, ReLU; BF16 operands, FP32 accumulation on the tensor cores)
+ * scores every candidate edge; aco_b200_apply_prior turns the scores s of
+ * row i into eta levels L = min(4095, round(gamma (max s - s) 16 / ln 2)),
+ * i.e. selection weights proportional to tau^alpha exp(gamma s), in place
+ * of the plain eta^beta = d^-beta levels.  gamma <= 0 (or prior NULL)
+ * restores the plain levels.  Training: softmax cross-entropy of each row's
+ * candidate slots against the successor an elite route takes (depot -> first
+ * customer, and both directions of every customer arc), Adam.
+ * Parameters: ACO_B200_PRIOR_PARAMS floats, W1[64][8], b1[64], W2[64][64],
+ * b2[64], w3[64], b3.  No counterpart in the reference.
+ */
+#define ACO_B200_PRIOR_PARAMS 4801
+typedef struct aco_b200_prior aco_b200_prior;
+
+/* Training set: instances packed like the batched problem (instance i
+ * occupies n[i]+1 entries of x, y, demand), plus one elite solution per
+ * instance in compact form (K[i] lengths, routes back to back). */
+typedef struct {
+  int count;
+  const int *n;
+  const int *K;
+  const long long *capacity;
+  const float *x, *y;
+  const int *demand;          /* NULL = unit demand */
+  const int *nodes;
+  const int *lens;
+  int cand_k;                 /* candidate list length, <= 32; 0 = 32 */
+} aco_b200_prior_dataset;
+
+ACO_API int aco_b200_prior_create(aco_b200_prior **out, int device);
+ACO_API int aco_b200_prior_destroy(aco_b200_prior *prior);
+ACO_API int aco_b200_prior_set_stream(aco_b200_prior *prior, void *cuda_stream);
+ACO_API int aco_b200_prior_init(aco_b200_prior *prior, unsigned int seed);
+ACO_API int aco_b200_prior_set_params(aco_b200_prior *prior, const float *params, int count);
+ACO_API int aco_b200_prior_get_params(aco_b200_prior *prior, float *params, int count);
+ACO_API int aco_b200_prior_load(aco_b200_prior *prior, const char *path);  /* raw float32 */
+ACO_API int aco_b200_prior_save(aco_b200_prior *prior, const char *path);
+ACO_API int aco_b200_prior_set_dataset(aco_b200_prior *prior,
+                                       const aco_b200_prior_dataset *data,
+                                       long long *n_examples);
+/* epochs over the training set in shuffled minibatches of `batch`
+ * examples; epoch_loss[epochs] (mean cross-entropy) may be NULL. */
+ACO_API int aco_b200_prior_train(aco_b200_prior *prior, int epochs, int batch, float lr,
+                                 unsigned int seed, float *epoch_loss);
+/* Test hooks: gradient (ACO_B200_PRIOR_PARAMS floats) and mean loss of the
+ * given examples; the examples as (feature row, target slot) pairs; feature
+ * rows (32 slots x 8 BF16 bit patterns each), their non-empty slot counts
+ * and (scores != NULL) the forward pass on them. */
+ACO_API int aco_b200_prior_gradient(aco_b200_prior *prior, const int *examples, int count,
+                                    float *grad, float *loss);
+ACO_API long long aco_b200_prior_num_examples(aco_b200_prior *prior);
+ACO_API int aco_b200_prior_get_examples(aco_b200_prior *prior, int *rows_slots, long long count);
+ACO_API int aco_b200_prior_get_rows(aco_b200_prior *prior, long long first, int count,
+                                    uint16_t *features, uint8_t *kv, float *scores);
+ACO_API int aco_b200_apply_prior(aco_b200_ctx *ctx, aco_b200_prior *prior, float gamma);
+
+/*
  * Batched solving: many independent instances in one persistent launch.
  * Each block takes instances from a queue and runs all their epochs itself
  * (weights, construction, best, evaporation, deposit), so instances of
@@ -221,6 +279,8 @@ ACO_API int aco_b200_batch_get(aco_b200_batch *batch, int instance, int *nodes, 
                                double *cost, int *epochs);
 ACO_API int aco_b200_batch_get_costs(aco_b200_batch *batch, double *costs, int *epochs,
                                      unsigned long long *steps);
+/* Learned eta levels for every instance of the batch (after setup). */
+ACO_API int aco_b200_batch_apply_prior(aco_b200_batch *batch, aco_b200_prior *prior, float gamma);
 
 /*
  * Evaporation then deposit without any device allocation, for callers that

@@ -39,6 +39,12 @@ EXPORTED = [
     "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
     "aco_b200_batch_get", "aco_b200_batch_get_costs",
     "aco_b200_shard_packet_ints", "aco_b200_shard_construct", "aco_b200_shard_update",
+    "aco_b200_prior_create", "aco_b200_prior_destroy", "aco_b200_prior_set_stream",
+    "aco_b200_prior_init", "aco_b200_prior_set_params", "aco_b200_prior_get_params",
+    "aco_b200_prior_load", "aco_b200_prior_save", "aco_b200_prior_set_dataset",
+    "aco_b200_prior_train", "aco_b200_prior_gradient", "aco_b200_prior_num_examples",
+    "aco_b200_prior_get_examples", "aco_b200_prior_get_rows", "aco_b200_apply_prior",
+    "aco_b200_batch_apply_prior",
     "aco_status_string", "aco_vrp_cuda_with_capacity", "aco_vrp_cuda_with_demands",
     "solution_create", "solution_free", "solution_reset", "solution_copy",
     "solution_cost", "route_append", "solution_validate",
@@ -130,11 +136,24 @@ def load():
         "aco_b200_batch_get_costs": [vp, vp, vp, vp],
         "aco_b200_shard_packet_ints": [vp], "aco_b200_shard_construct": [vp, vp],
         "aco_b200_shard_update": [vp, vp, i32],
+        "aco_b200_prior_create": [vp, i32], "aco_b200_prior_destroy": [vp],
+        "aco_b200_prior_set_stream": [vp, vp], "aco_b200_prior_init": [vp, C.c_uint],
+        "aco_b200_prior_set_params": [vp, vp, i32], "aco_b200_prior_get_params": [vp, vp, i32],
+        "aco_b200_prior_load": [vp, C.c_char_p], "aco_b200_prior_save": [vp, C.c_char_p],
+        "aco_b200_prior_set_dataset": [vp, vp, vp],
+        "aco_b200_prior_train": [vp, i32, i32, f32, C.c_uint, vp],
+        "aco_b200_prior_gradient": [vp, vp, i32, vp, vp],
+        "aco_b200_prior_get_examples": [vp, vp, C.c_longlong],
+        "aco_b200_prior_get_rows": [vp, C.c_longlong, i32, vp, vp, vp],
+        "aco_b200_apply_prior": [vp, vp, f32],
+        "aco_b200_batch_apply_prior": [vp, vp, f32],
     }
     for name, args in sigs.items():
         fn = getattr(L, name)
         fn.argtypes = args
         fn.restype = i32
+    L.aco_b200_prior_num_examples.argtypes = [vp]
+    L.aco_b200_prior_num_examples.restype = C.c_longlong
     L.aco_b200_build_info.restype = C.c_char_p
     L.aco_status_string.restype = C.c_char_p
     L.aco_status_string.argtypes = [i32]
@@ -323,6 +342,126 @@ class Context:
         _check(self._lib.aco_b200_shard_update(self._h, C.c_void_p(d_recv), world),
                "aco_b200_shard_update")
 
+    def apply_prior(self, prior: Optional["Prior"], gamma: float = 1.0) -> None:
+        """Learned eta levels from `prior` (None or gamma <= 0: plain levels)."""
+        _check(self._lib.aco_b200_apply_prior(self._h, prior._h if prior else None, gamma),
+               "aco_b200_apply_prior")
+
+
+PRIOR_PARAMS = 4801
+
+
+class PriorDataset(C.Structure):
+    _fields_ = [("count", C.c_int), ("n", C.c_void_p), ("K", C.c_void_p),
+                ("capacity", C.c_void_p), ("x", C.c_void_p), ("y", C.c_void_p),
+                ("demand", C.c_void_p), ("nodes", C.c_void_p), ("lens", C.c_void_p),
+                ("cand_k", C.c_int)]
+
+
+class Prior:
+    """Learned heuristic prior (aco_b200_prior): MLP parameters, training set,
+    tensor-core training and inference."""
+
+    def __init__(self, device: int = 0, seed: Optional[int] = None):
+        self._lib = load()
+        self._h = C.c_void_p()
+        _check(self._lib.aco_b200_prior_create(C.byref(self._h), device), "aco_b200_prior_create")
+        if seed is not None:
+            self.init(seed)
+
+    def close(self):
+        if self._h:
+            self._lib.aco_b200_prior_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def init(self, seed: int) -> None:
+        _check(self._lib.aco_b200_prior_init(self._h, seed & 0xffffffff), "aco_b200_prior_init")
+
+    def set_params(self, params) -> None:
+        p = np.ascontiguousarray(params, np.float32)
+        assert p.size == PRIOR_PARAMS
+        _check(self._lib.aco_b200_prior_set_params(self._h, _p(p), PRIOR_PARAMS),
+               "aco_b200_prior_set_params")
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(PRIOR_PARAMS, np.float32)
+        _check(self._lib.aco_b200_prior_get_params(self._h, _p(p), PRIOR_PARAMS),
+               "aco_b200_prior_get_params")
+        return p
+
+    def save(self, path: str) -> None:
+        _check(self._lib.aco_b200_prior_save(self._h, path.encode()), "aco_b200_prior_save")
+
+    def load(self, path: str) -> None:
+        _check(self._lib.aco_b200_prior_load(self._h, path.encode()), "aco_b200_prior_load")
+
+    def set_dataset(self, instances, solutions, cand_k: int = 32) -> int:
+        """instances: list of Instance; solutions: list of (nodes, lens) in
+        compact form.  Returns the number of training examples."""
+        n = np.array([x.n for x in instances], np.int32)
+        K = np.array([x.vehicles for x in instances], np.int32)
+        cap = np.array([x.capacity for x in instances], np.int64)
+        xs = np.concatenate([x.x for x in instances]).astype(np.float32)
+        ys = np.concatenate([x.y for x in instances]).astype(np.float32)
+        dem = np.concatenate([x.demand for x in instances]).astype(np.int32)
+        nodes = np.concatenate([np.asarray(s[0], np.int32) for s in solutions])
+        lens = np.concatenate([np.asarray(s[1], np.int32) for s in solutions])
+        keep = [n, K, cap, xs, ys, dem, nodes, lens]
+        d = PriorDataset(count=len(instances), n=_p(n).value, K=_p(K).value, capacity=_p(cap).value,
+                         x=_p(xs).value, y=_p(ys).value, demand=_p(dem).value,
+                         nodes=_p(nodes).value, lens=_p(lens).value, cand_k=cand_k)
+        cnt = C.c_longlong()
+        _check(self._lib.aco_b200_prior_set_dataset(self._h, C.byref(d), C.byref(cnt)),
+               "aco_b200_prior_set_dataset")
+        del keep
+        return cnt.value
+
+    def num_examples(self) -> int:
+        return int(self._lib.aco_b200_prior_num_examples(self._h))
+
+    def examples(self) -> np.ndarray:
+        cnt = self.num_examples()
+        e = np.zeros(2 * max(cnt, 1), np.int32)
+        _check(self._lib.aco_b200_prior_get_examples(self._h, _p(e), cnt),
+               "aco_b200_prior_get_examples")
+        return e[: 2 * cnt].reshape(cnt, 2)
+
+    def rows(self, first: int, count: int, scores: bool = False):
+        """(features [count][32][8] BF16 bit patterns, kv [count],
+        scores [count][32] or None)."""
+        f = np.zeros(count * 32 * 8, np.uint16)
+        kv = np.zeros(count, np.uint8)
+        sc = np.zeros(count * 32, np.float32) if scores else None
+        _check(self._lib.aco_b200_prior_get_rows(self._h, first, count, _p(f), _p(kv), _p(sc)),
+               "aco_b200_prior_get_rows")
+        return f.reshape(count, 32, 8), kv, None if sc is None else sc.reshape(count, 32)
+
+    def gradient(self, example_ids):
+        ids = np.ascontiguousarray(example_ids, np.int32)
+        g = np.zeros(PRIOR_PARAMS, np.float32)
+        loss = C.c_float()
+        _check(self._lib.aco_b200_prior_gradient(self._h, _p(ids), len(ids), _p(g),
+                                                 C.byref(loss)), "aco_b200_prior_gradient")
+        return float(loss.value), g
+
+    def train(self, epochs: int, batch: int = 2048, lr: float = 1e-3, seed: int = 0):
+        losses = np.zeros(max(epochs, 1), np.float32)
+        _check(self._lib.aco_b200_prior_train(self._h, epochs, batch, lr, seed & 0xffffffff,
+                                              _p(losses)), "aco_b200_prior_train")
+        return losses[:epochs]
+
 
 class BatchProblem(C.Structure):
     _fields_ = [("count", C.c_int), ("n", C.c_void_p), ("K", C.c_void_p),
@@ -435,6 +574,10 @@ class Batch:
             return nodes[:0], lens, float("inf"), ep.value
         _check(rc, "aco_b200_batch_get")
         return nodes[: int(lens.sum())].copy(), lens, cost.value, ep.value
+
+    def apply_prior(self, prior: Optional[Prior], gamma: float = 1.0) -> None:
+        _check(self._lib.aco_b200_batch_apply_prior(self._h, prior._h if prior else None, gamma),
+               "aco_b200_batch_apply_prior")
 
     def costs(self):
         c = np.zeros(self.count, np.float64)

@@ -9,6 +9,7 @@
 // the single-instance path solves it with seed + i (same draws, same rules,
 // same device math), which the tests check route for route.
 #include "aco_internal.cuh"
+#include "aco_prior_internal.h"
 
 extern "C" {
 #include "aco.h"
@@ -611,6 +612,7 @@ struct aco_b200_batch {
   void *bufs[32] = {nullptr};
   int nbufs = 0;
   aco_b200_batch_tuning tuning = {32, 16, 1};
+  const float *d_thr = nullptr;  // eta thresholds (plain levels)
   void free_all() {
     for (int i = 0; i < nbufs; ++i) cudaFree(bufs[i]);
     nbufs = 0;
@@ -851,6 +853,7 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
   for (int i = 0; i < count; ++i)
     BTRY(launch_knn_levels(d_coords + b->inst[i].node_off, b->inst[i].n, k, d_thr, kThresholds,
                            d_cand + b->inst[i].node_off * k, d_lvl + b->inst[i].node_off * k, s));
+  b->d_thr = d_thr;
   a.inst = d_inst;
   a.order = d_order;
   a.coords = d_coords;
@@ -994,3 +997,26 @@ int aco_b200_batch_get_costs(aco_b200_batch *b, double *costs, int *epochs,
 }
 
 }  // extern "C"
+
+extern "C" int aco_b200_batch_apply_prior(aco_b200_batch *b, aco_b200_prior *prior, float gamma) {
+  if (!b || !b->ready) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(b->device);
+  cudaStream_t s = b->stream;
+  const BatchArgs &a = b->args;
+  uint16_t *lvl = const_cast<uint16_t *>(a.lvl);
+  for (int i = 0; i < b->count; ++i) {
+    const BatchInst &I = b->inst[i];
+    if (prior && gamma > 0.f) {
+      int rc = acob200::prior::learned_levels(prior, a.coords + I.node_off, a.demand + I.node_off,
+                                              I.cap, I.n, b->k, a.cand + I.node_off * b->k,
+                                              lvl + I.node_off * b->k, gamma, s);
+      if (rc) return rc;
+    } else {
+      BTRY(launch_knn_levels(a.coords + I.node_off, I.n, b->k, b->d_thr, kThresholds,
+                             const_cast<uint16_t *>(a.cand) + I.node_off * b->k,
+                             lvl + I.node_off * b->k, s));
+    }
+  }
+  BTRY(cudaStreamSynchronize(s));
+  return ACO_OK;
+}

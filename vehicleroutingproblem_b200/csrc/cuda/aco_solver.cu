@@ -3,6 +3,7 @@
 // CUDA-graph chunks, and the reference-facing aco_vrp_cuda_with_capacity
 // (src/cuda/aco_cuda.cu:188-454) with its progress output.
 #include "aco_internal.cuh"
+#include "aco_prior_internal.h"
 
 extern "C" {
 #include "aco.h"
@@ -527,6 +528,22 @@ int aco_b200_enqueue_epochs(aco_b200_ctx *ctx, int epochs) {
     left -= kChunkEpochs;
   }
   for (int i = 0; i < left; ++i) TRY(cudaGraphLaunch(ctx->graph_one, s));
+  return ACO_OK;
+}
+
+int aco_b200_apply_prior(aco_b200_ctx *ctx, aco_b200_prior *prior, float gamma) {
+  if (!ctx || !ctx->ready) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  if (prior && gamma > 0.f) {
+    int rc = acob200::prior::learned_levels(prior, ctx->d_coords, ctx->d_demand, ctx->cap, ctx->n,
+                                            ctx->k, ctx->d_cand, ctx->d_lvl, gamma, s);
+    if (rc) return rc;
+  } else {
+    TRY(launch_knn_levels(ctx->d_coords, ctx->n, ctx->k, ctx->d_thr, kThresholds, ctx->d_cand,
+                          ctx->d_lvl, s));
+  }
+  TRY(cudaStreamSynchronize(s));
   return ACO_OK;
 }
 

@@ -1,7 +1,7 @@
 """Benchmark of the ACO-for-CVRP hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload n1000|small|clustered2000|batched]
+                    [--workload n1000|small|clustered2000|batched|learned]
 
 Default workload (n1000): n=1000, K=8 uniform integer coordinates in
 [0,1000]^2 from seed 19001, depot (500,500), demands uniform in [1,100],
@@ -13,6 +13,8 @@ clustered2000: n=2000, K=16, 70% in 8 Gaussian clusters, 1024 ants, 32-NN.
 batched: 512 instances (n~U[50,500], K=ceil(n/60), seeds 30000-30511), 64
 ants, 16-NN, 300 epochs each, all in one persistent launch; a step is one
 solve of the whole batch and the metric is instances/s.
+learned: the learned prior's time-to-cost against plain eta on 256 held-out
+n=1000 instances (training set, training and evaluation inside the run).
 
 * value: device time (CUDA events on the library's stream), L2 flushed by a
   256 MiB write between steps outside the events, all ranks' work over the
@@ -634,6 +636,88 @@ def run_batched(args, rank, world, local, torch, dist, _native):
     return line
 
 
+LEARNED = dict(train=4096, heldout=256, elite_ants=64, elite_k=16, elite_epochs=120,
+               train_epochs=10, batch=4096, lr=2e-3, gammas=(1.0, 2.0, 4.0), validation=8,
+               epochs=300, ants=256, cand_k=32,
+               name="learned prior: 4096 training instances n~U[200,1000] (seed 40000), "
+                    "256 held-out n=1000 K=8 (seeds 50000-50255), 256 ants 32-NN, "
+                    "300 epochs, target = plain final cost +0.5%")
+# Useful FLOPs per candidate edge of one training step: forward
+# 2 (8*64 + 64*64 + 64), backward 2 (64*64 + 64*64 + 8*64 + 64).
+TRAIN_FLOPS_PER_EDGE = 2 * (8 * 64 + 64 * 64 + 64) + 2 * (64 * 64 + 64 * 64 + 8 * 64 + 64)
+
+
+def run_learned(args, rank, world, local, torch, dist, _native):
+    """Time-to-cost of the learned prior against plain eta on held-out
+    instances (one GPU; the whole pipeline -- elite routes by the plain
+    batched solver, training set, tensor-core training, gamma chosen on 8
+    validation instances, evaluation -- runs inside this call)."""
+    from vehicleroutingproblem_b200 import prior as PR
+    if rank != 0:
+        return None
+    L = LEARNED
+    ntrain = args.prior_train or L["train"]
+    nheld = args.prior_heldout or L["heldout"]
+    tr = I.prior_training_instances(ntrain)
+    t0 = time.perf_counter()
+    sols = PR.elite_solutions(tr, ants=L["elite_ants"], cand_k=L["elite_k"],
+                              epochs=L["elite_epochs"])
+    elite_s = time.perf_counter() - t0
+    pr = _native.Prior(local, seed=1)
+    t0 = time.perf_counter()
+    count = pr.set_dataset(tr, [(s[0], s[1]) for s in sols], cand_k=L["cand_k"])
+    dataset_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    losses = pr.train(L["train_epochs"], batch=L["batch"], lr=L["lr"], seed=11)
+    train_s = time.perf_counter() - t0
+    val = [I.uniform_instance(1000, 8, 60000 + i) for i in range(L["validation"])]
+    scores = {}
+    for g in L["gammas"]:
+        r = PR.time_to_cost(val, pr, gamma=g, epochs=L["epochs"], ants=L["ants"],
+                            cand_k=L["cand_k"])
+        scores[g] = r["time_ratio_of_sums"]
+    gamma = min(scores, key=lambda g: scores[g])
+    held = I.prior_heldout_instances(nheld)
+    t0 = time.perf_counter()
+    res = PR.time_to_cost(held, pr, gamma=gamma, epochs=L["epochs"], ants=L["ants"],
+                          cand_k=L["cand_k"])
+    eval_s = time.perf_counter() - t0
+    rows = res.pop("rows")
+    flops = TRAIN_FLOPS_PER_EDGE * 32.0 * count * L["train_epochs"]
+    peak, peak_kind = None, "fallback"
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = float(json.load(f)["bf16_tflops"])  # burst: short launches
+        peak_kind = "measured"
+    except Exception:
+        peak = 1590.0
+    achieved = flops / train_s / 1e12
+    line = {
+        "metric": "time-to-cost ratio (learned / plain eta)", "value": res["time_ratio_of_sums"],
+        "unit": "ratio", "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 MLP (fp32 accumulate) + int32 weights + u8 pheromone",
+        "data": "synthetic",
+        "config": {"workload": L["name"], "train_instances": ntrain, "heldout": nheld,
+                   "gamma": gamma, "gamma_validation": scores},
+        "time_to_cost": res,
+        "training": {"examples": count, "epochs": L["train_epochs"], "batch": L["batch"],
+                     "lr": L["lr"], "loss_first_last": [float(losses[0]), float(losses[-1])],
+                     "elite_s": elite_s, "dataset_s": dataset_s, "train_s": train_s,
+                     "examples_per_s": count * L["train_epochs"] / train_s},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "k_prior_mlp<train> with reduce, Adam and the per-epoch "
+                               "shuffle upload (host-timed)",
+                     "flops_per_edge": TRAIN_FLOPS_PER_EDGE},
+        "eval_s": eval_s,
+        "per_instance_sample": rows[:4],
+    }
+    pr.close()
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -641,7 +725,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="n1000",
-                    choices=sorted(WORKLOADS) + ["batched"])
+                    choices=sorted(WORKLOADS) + ["batched", "learned"])
+    ap.add_argument("--prior-train", type=int, default=None,
+                    help="learned: training instances (default 4096)")
+    ap.add_argument("--prior-heldout", type=int, default=None,
+                    help="learned: held-out instances (default 256)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--looped-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -662,6 +750,12 @@ def main():
     rank, world, local = dist_env()
 
     if args.impl == "reference":
+        if args.workload == "learned":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable":
+                                  "the reference has no learned prior; its plain eta solver is "
+                                  "the denominator of this workload's ratio"}), flush=True)
+            return 0
         return run_reference_arm(args, rank, world)
 
     import datetime
@@ -671,7 +765,8 @@ def main():
     from vehicleroutingproblem_b200 import _native
 
     torch.cuda.set_device(local)
-    sharded = not batched and (world > 1 or args.colony == "sharded")
+    learned = args.workload == "learned"
+    sharded = not batched and not learned and (world > 1 or args.colony == "sharded")
     pg = world > 1 or sharded
     if world > 1:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
@@ -685,7 +780,8 @@ def main():
                                 world_size=1, timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     try:
-        fn = run_batched if batched else (run_sharded if sharded else run_single)
+        fn = (run_batched if batched else run_learned if learned else
+              run_sharded if sharded else run_single)
         line = fn(args, rank, world, local, torch, dist, _native)
         if line is not None:
             print(json.dumps(line), flush=True)

@@ -194,3 +194,44 @@ def test_batch_levels_equal_context_levels(dataset, native):
                 bn, bl, bc, be = b.best(i)
                 nodes, lens, cost = c.best()
                 assert bc == cost and np.array_equal(bn, nodes) and np.array_equal(bl, lens)
+
+
+def test_cli_learned_prior_and_plain_fallback(dataset, tmp_path):
+    import os
+    import subprocess
+    _, _, pr, _, _ = dataset
+    cli = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                       "aco_vrp_cuda.out")
+    params = tmp_path / "prior.bin"
+    pr.save(str(params))
+    inst = I.uniform_instance(60, 3, 816)
+    vrp = tmp_path / "i.vrp"
+    I.write_vrp(inst, str(vrp))
+    env = dict(os.environ, ACO_SOLVER_FIXED_EPOCHS="20", ACO_SOLVER_STAGNATION_EPOCHS="0",
+               ACO_SOLVER_PROGRESS_INTERVAL_SECONDS="0", ACO_CUDA_PRIOR="learned",
+               ACO_CUDA_PRIOR_FILE=str(params))
+    r = subprocess.run([cli, str(vrp), "3", "32", "5"], env=env, capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 0 and "best cost:" in r.stdout, r.stderr
+    assert "unavailable" not in r.stderr
+    env["ACO_CUDA_PRIOR_FILE"] = str(tmp_path / "missing.bin")
+    r2 = subprocess.run([cli, str(vrp), "3", "32", "5"], env=env, capture_output=True,
+                        text=True, timeout=120)
+    assert r2.returncode == 0 and "best cost:" in r2.stdout
+    assert "learned prior unavailable" in r2.stderr
+    env["ACO_CUDA_PRIOR"] = "plain"
+    r3 = subprocess.run([cli, str(vrp), "3", "32", "5"], env=env, capture_output=True,
+                        text=True, timeout=120)
+    # a missing file falls back to exactly the plain solver
+    assert r3.returncode == 0
+    assert r3.stdout.split("best cost:")[1] == r2.stdout.split("best cost:")[1]
+
+
+def test_time_to_cost_pipeline(dataset):
+    from vehicleroutingproblem_b200 import prior as PR
+    _, _, pr, _, _ = dataset
+    res = PR.time_to_cost([I.uniform_instance(150, 3, 817)], pr, gamma=1.0, epochs=30,
+                          ants=32, cand_k=32)
+    row = res["rows"][0]
+    assert res["instances"] == 1 and 1 <= row["plain_epochs"] <= 30
+    assert row["plain_s"] > 0 and row["learned_s"] > 0 and row["prior_s"] > 0

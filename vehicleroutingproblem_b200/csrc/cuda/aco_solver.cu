@@ -801,6 +801,37 @@ static void print_progress(int epoch, double elapsed_s, double max_runtime_s,
   fflush(stdout);
 }
 
+// ACO_CUDA_PRIOR=learned with ACO_CUDA_PRIOR_FILE (ACO_B200_PRIOR_PARAMS raw
+// float32 values) and ACO_CUDA_PRIOR_GAMMA (default 2): learned eta levels.
+// Any failure keeps the plain levels, with a note on stderr.
+static void apply_prior_from_env(aco_b200_ctx *ctx) {
+  const char *mode = getenv("ACO_CUDA_PRIOR");
+  if (!mode || !*mode || strcmp(mode, "plain") == 0) return;
+  if (strcmp(mode, "learned") != 0) {
+    fprintf(stderr, "[cuda] ACO_CUDA_PRIOR=%s not recognised (plain|learned): plain eta\n", mode);
+    return;
+  }
+  const char *file = getenv("ACO_CUDA_PRIOR_FILE");
+  float gamma = 2.0f;
+  const char *g = getenv("ACO_CUDA_PRIOR_GAMMA");
+  if (g && *g) {
+    char *end = nullptr;
+    const double v = strtod(g, &end);
+    if (end && *end == '\0' && v > 0.0 && v < 1e6) gamma = (float)v;
+    else fprintf(stderr, "[cuda] ACO_CUDA_PRIOR_GAMMA=%s ignored\n", g);
+  }
+  aco_b200_prior *prior = nullptr;
+  int rc = file && *file ? aco_b200_prior_create(&prior, ctx->device) : ACO_ERR_INVALID_INPUT;
+  if (rc == ACO_OK) rc = aco_b200_prior_load(prior, file);
+  if (rc == ACO_OK) rc = aco_b200_apply_prior(ctx, prior, gamma);
+  if (rc != ACO_OK) {
+    fprintf(stderr, "[cuda] learned prior unavailable (%s, file %s): plain eta\n",
+            aco_status_string((AcoStatus)rc), file ? file : "not set");
+    aco_b200_apply_prior(ctx, nullptr, 0.f);
+  }
+  if (prior) aco_b200_prior_destroy(prior);
+}
+
 static AcoStatus solve_impl(int n, int K, long long capacity, int m,
                             const float *x, const float *y, const int *demand,
                             double alpha, double beta, double rho, double tau0,
@@ -839,6 +870,7 @@ static AcoStatus solve_impl(int n, int K, long long capacity, int m,
     aco_b200_destroy(ctx);
     return (AcoStatus)rc;
   }
+  apply_prior_from_env(ctx);
   printf("CUDA Solver starting... (N=%d, K=%d, M=%d)\n", n, K, m);
   const double start = wall_seconds();
   double next_report = cfg.progress_interval_seconds > 0.0 ? start + cfg.progress_interval_seconds : 0.0;

@@ -147,6 +147,27 @@ def workload_clustered2000(seed: int = 29001) -> Instance:
                               name=f"c3_n2000_k16_s{seed}")
 
 
+def prior_training_instances(count: int = 4096, seed0: int = 40000) -> List[Instance]:
+    """Training set of the learned prior: n ~ U[200,1000] (drawn from seed0),
+    K = ceil(n/125), demands [1,100]; even indices uniform, odd clustered;
+    instance i uses seed seed0 + 1 + i."""
+    rs = np.random.RandomState(seed0)
+    ns = rs.randint(200, 1001, size=count)
+    out = []
+    for i, n in enumerate(ns):
+        n = int(n)
+        K = int(math.ceil(n / 125))
+        make = uniform_instance if i % 2 == 0 else clustered_instance
+        out.append(make(n, K, seed0 + 1 + i))
+    return out
+
+
+def prior_heldout_instances(count: int = 256, seed0: int = 50000) -> List[Instance]:
+    """Held-out evaluation set of the learned prior: n=1000, K=8, uniform,
+    demands [1,100] (the n1000 workload's shape), seeds seed0 .. seed0+count-1."""
+    return [uniform_instance(1000, 8, seed0 + i) for i in range(count)]
+
+
 # --------------------------------------------------------------------------
 # TSPLIB text
 # --------------------------------------------------------------------------

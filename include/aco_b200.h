@@ -59,6 +59,9 @@ typedef struct {
   double timeout_seconds;     /* 0 = none                                  */
   int ant_base;               /* global id of ant 0 (colony split over
                                  devices); 0 for a whole colony            */
+  int depot_rule;             /* 0 = sequential path's rule (default);
+                                 1 = reference CUDA kernel's stochastic
+                                 depot close, aco_cuda_kernels.cu:487-520 */
 } aco_b200_problem;
 
 /* Device-side solver state after a run. */
@@ -128,6 +131,10 @@ ACO_API int aco_b200_get_tables(aco_b200_ctx *ctx, int32_t *A, uint32_t *lut,
                         float *thresholds, int n_thresholds);
 /* Weights recomputed from the current pheromone ((n+1) k values). */
 ACO_API int aco_b200_get_weights(aco_b200_ctx *ctx, uint32_t *w);
+/* Depot rule 1 only: eta level of d(i,0)^2 per node, the last weights
+ * pass's depot-close levels rdep[n+1] and the depot factor's level e_dep. */
+ACO_API int aco_b200_get_depot_tables(aco_b200_ctx *ctx, uint16_t *lvl0, int32_t *rdep,
+                                      int *e_dep);
 /* One construct pass for epoch number `epoch` on the current pheromone;
  * per-ant results through aco_b200_get_ants.  layout: -1 = automatic,
  * 0 = shared-memory weights, 1 = shared-memory packed levels, 2 = global. */

@@ -320,6 +320,51 @@ ORC_EXPORT double orc_route_cost(const float *x, const float *y,
   return cost;
 }
 
+/* Reference-CUDA depot rule (kernel_construct_solutions,
+ * src/cuda/aco_cuda_kernels.cu:487-520), restated on the integer weights.
+ * The reference weighs closing the route against the candidates by
+ * 2 (1/(d0+eps))^beta versus tau^alpha eta^beta; in 1/16-octave levels the
+ * close level of row i is e_dep - lvl0[i] (e_dep = 16 (1 - alpha log2 tau_min),
+ * lvl0 = eta level of d(i,0)^2) and, on the row's weight scale,
+ * rdep[i] = emax_i - (e_dep - lvl0[i]) levels below the row maximum. */
+ORC_EXPORT void orc_depot_rel(int n, int k, const int32_t *cand, const uint16_t *lvl,
+                              const uint8_t *tau, const int32_t *A, const uint16_t *lvl0,
+                              int32_t e_dep, int32_t *rdep) {
+  size_t stride = (size_t)n + 1;
+  for (int i = 0; i <= n; ++i) {
+    int have = 0;
+    int32_t emax = 0;
+    for (int t = 0; t < k; ++t) {
+      int c = cand[(size_t)i * k + t];
+      if (c <= 0) continue;
+      int32_t e = A[tau[(size_t)i * stride + c]] - (int32_t)lvl[(size_t)i * k + t];
+      if (!have || e > emax) emax = e;
+      have = 1;
+    }
+    rdep[i] = have ? emax - (e_dep - (int32_t)lvl0[i]) : 0;
+  }
+}
+
+/* Close weight 2^23 2^(-r/16) on the row's weight scale, exact in FP64:
+ * LUT[r mod 16] 2^(-floor(r/16)); 0 from r = 255 on. */
+static double depot_weight(int32_t r, const uint32_t *lut) {
+  if (r >= ORC_REL_MAX) return 0.0;
+  int32_t q = (r >= 0) ? (r / 16) : -((-r + 15) / 16);
+  return ldexp((double)lut[r - 16 * q], -q);
+}
+
+typedef struct {
+  int rule;              /* 0 sequential path, 1 reference CUDA kernel */
+  const int32_t *rdep;   /* rule 1: [(n+1)] */
+  const uint32_t *lut;   /* rule 1: [256] */
+} OrcRule;
+
+static int construct_ant(int n, int K, int k, int64_t cap, const float *x, const float *y,
+                         const int32_t *demand, const int32_t *cand, const uint32_t *w,
+                         uint32_t seed, uint32_t epoch, uint32_t ant, uint32_t stream,
+                         const OrcRule *rule, int32_t *nodes_out, int32_t *lens_out,
+                         double *cost_out, int32_t *steps_out, uint32_t *draws_out);
+
 /* build_ant_solution, aco_sequential.c:616-681.  Writes the compact route
  * (capacity n + 2K), the K lengths, the FP64 cost and the number of moves
  * (customers plus depot returns).  Returns 1 if every customer is served. */
@@ -331,6 +376,55 @@ ORC_EXPORT int orc_construct_ant(int n, int K, int k, int64_t cap,
                                  int32_t *nodes_out, int32_t *lens_out,
                                  double *cost_out, int32_t *steps_out,
                                  uint32_t *draws_out) {
+  OrcRule r = {0, NULL, NULL};
+  return construct_ant(n, K, k, cap, x, y, demand, cand, w, seed, epoch, ant, stream, &r,
+                       nodes_out, lens_out, cost_out, steps_out, draws_out);
+}
+
+/* The same with the reference-CUDA depot rule (rule 1): vehicle v extends
+ * while customers remain and load < Q; once the remaining demand fits the
+ * later vehicles the route may close -- at the depot at once, with no
+ * eligible candidate at once, and after a roulette draw when a second draw
+ * u satisfies u (denom + w_depot) >= denom (FP64, u = r / 2^24). */
+ORC_EXPORT int orc_construct_ant_rule(int n, int K, int k, int64_t cap,
+                                      const float *x, const float *y,
+                                      const int32_t *demand, const int32_t *cand,
+                                      const uint32_t *w, uint32_t seed,
+                                      uint32_t epoch, uint32_t ant, uint32_t stream,
+                                      int rule, const int32_t *rdep, const uint32_t *lut,
+                                      int32_t *nodes_out, int32_t *lens_out,
+                                      double *cost_out, int32_t *steps_out,
+                                      uint32_t *draws_out) {
+  OrcRule r = {rule, rdep, lut};
+  return construct_ant(n, K, k, cap, x, y, demand, cand, w, seed, epoch, ant, stream, &r,
+                       nodes_out, lens_out, cost_out, steps_out, draws_out);
+}
+
+/* A step of the reference-CUDA rule where the route may close: no eligible
+ * candidate closes it; otherwise the roulette draw picks a candidate and a
+ * second draw decides whether the route closes instead (returns 0). */
+static int select_close(OrcAnt *a, int cur, int64_t load, const OrcRule *rule) {
+  const int32_t *crow = a->cand + (size_t)cur * a->k;
+  const uint32_t *wrow = a->w + (size_t)cur * a->k;
+  uint64_t denom = 0;
+  for (int t = 0; t < a->k; ++t) {
+    int c = crow[t];
+    if (c <= 0 || vis_get(a->visited, c) || load + dem(a, c) > a->cap) continue;
+    denom += wrow[t];
+  }
+  if (denom == 0) return 0;
+  int next = select_next(a, cur, load);  /* consumes the roulette draw */
+  uint64_t r2 = orc_draw24(a->seed, a->epoch, a->ant, a->stream, a->draws++);
+  double wd = depot_weight(rule->rdep[cur], rule->lut);
+  if ((double)r2 * ((double)denom + wd) >= (double)denom * 16777216.0) return 0;
+  return next;
+}
+
+static int construct_ant(int n, int K, int k, int64_t cap, const float *x, const float *y,
+                         const int32_t *demand, const int32_t *cand, const uint32_t *w,
+                         uint32_t seed, uint32_t epoch, uint32_t ant, uint32_t stream,
+                         const OrcRule *rule, int32_t *nodes_out, int32_t *lens_out,
+                         double *cost_out, int32_t *steps_out, uint32_t *draws_out) {
   int words = n / 64 + 1;
   uint64_t *visited = (uint64_t *)calloc((size_t)words, sizeof(uint64_t));
   int32_t *routes = (int32_t *)malloc(sizeof(int32_t) * (size_t)K * (size_t)(n + 2));
@@ -347,8 +441,15 @@ ORC_EXPORT int orc_construct_ant(int n, int K, int k, int64_t cap,
     r[rlen[v]++] = 0;
     int cur = 0;
     int64_t future = (int64_t)(K - v - 1) * a.cap;
-    while (remaining > 0 && rem_dem > future && loads[v] < a.cap) {
-      int next = select_next(&a, cur, loads[v]);
+    int64_t limit = rule->rule == 1 ? 0 : future;
+    while (remaining > 0 && rem_dem > limit && loads[v] < a.cap) {
+      int next;
+      if (rule->rule == 1 && rem_dem <= future) {
+        if (cur == 0) break;
+        next = select_close(&a, cur, loads[v], rule);
+      } else {
+        next = select_next(&a, cur, loads[v]);
+      }
       if (next <= 0 || vis_get(visited, next)) break;
       r[rlen[v]++] = next;
       vis_set(visited, next);

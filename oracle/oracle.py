@@ -56,6 +56,11 @@ def lib():
         L.orc_construct_ant.argtypes = [i32, i32, i32, i64, vp, vp, vp, vp, vp,
                                         u32, u32, u32, u32, vp, vp, vp, vp, vp]
         L.orc_construct_ant.restype = i32
+        L.orc_construct_ant_rule.argtypes = [i32, i32, i32, i64, vp, vp, vp, vp, vp,
+                                             u32, u32, u32, u32, i32, vp, vp,
+                                             vp, vp, vp, vp, vp]
+        L.orc_construct_ant_rule.restype = i32
+        L.orc_depot_rel.argtypes = [i32, i32, vp, vp, vp, vp, vp, C.c_int32, vp]
         L.orc_evaporate.argtypes = [vp, C.c_uint64, C.c_uint8, C.c_uint8]
         L.orc_deposit_level.argtypes = [C.c_uint8, f32, f32, f32, C.c_uint8, C.c_uint8]
         L.orc_deposit_level.restype = C.c_uint8
@@ -145,9 +150,21 @@ def weights(n, k, cand, lvl, tau, A, lut) -> np.ndarray:
     return w
 
 
+def depot_rel(n, k, cand, lvl, tau, A, lvl0, e_dep) -> np.ndarray:
+    """Depot-close levels of the reference-CUDA depot rule, per row."""
+    out = np.zeros(n + 1, dtype=np.int32)
+    lib().orc_depot_rel(n, k, _p(np.ascontiguousarray(cand, np.int32)),
+                        _p(np.ascontiguousarray(lvl, np.uint16)),
+                        _p(np.ascontiguousarray(tau, np.uint8)),
+                        _p(np.ascontiguousarray(A, np.int32)),
+                        _p(np.ascontiguousarray(lvl0, np.uint16)), int(e_dep), _p(out))
+    return out
+
+
 def construct_ant(inst_x, inst_y, demand, K, cap, k, cand, w, seed, epoch, ant,
-                  stream=0):
-    """Returns (feasible, nodes, lens, cost, steps, draws_used)."""
+                  stream=0, rule=0, rdep=None, lut=None):
+    """Returns (feasible, nodes, lens, cost, steps, draws_used).  rule 1 is
+    the reference-CUDA depot rule (needs rdep and the weight LUT)."""
     n = len(inst_x) - 1
     nodes = np.zeros(n + 2 * K, dtype=np.int32)
     lens = np.zeros(K, dtype=np.int32)
@@ -155,12 +172,21 @@ def construct_ant(inst_x, inst_y, demand, K, cap, k, cand, w, seed, epoch, ant,
     steps = C.c_int32()
     used = C.c_uint32()
     dem = None if demand is None else np.ascontiguousarray(demand, np.int32)
-    feas = lib().orc_construct_ant(
-        n, K, k, int(cap), _p(np.ascontiguousarray(inst_x, np.float32)),
-        _p(np.ascontiguousarray(inst_y, np.float32)), _p(dem),
-        _p(np.ascontiguousarray(cand, np.int32)), _p(np.ascontiguousarray(w, np.uint32)),
-        seed, epoch, ant, stream, _p(nodes), _p(lens), C.byref(cost), C.byref(steps),
-        C.byref(used))
+    if rule == 0:
+        feas = lib().orc_construct_ant(
+            n, K, k, int(cap), _p(np.ascontiguousarray(inst_x, np.float32)),
+            _p(np.ascontiguousarray(inst_y, np.float32)), _p(dem),
+            _p(np.ascontiguousarray(cand, np.int32)), _p(np.ascontiguousarray(w, np.uint32)),
+            seed, epoch, ant, stream, _p(nodes), _p(lens), C.byref(cost), C.byref(steps),
+            C.byref(used))
+    else:
+        feas = lib().orc_construct_ant_rule(
+            n, K, k, int(cap), _p(np.ascontiguousarray(inst_x, np.float32)),
+            _p(np.ascontiguousarray(inst_y, np.float32)), _p(dem),
+            _p(np.ascontiguousarray(cand, np.int32)), _p(np.ascontiguousarray(w, np.uint32)),
+            seed, epoch, ant, stream, int(rule), _p(np.ascontiguousarray(rdep, np.int32)),
+            _p(np.ascontiguousarray(lut, np.uint32)), _p(nodes), _p(lens), C.byref(cost),
+            C.byref(steps), C.byref(used))
     total = int(lens.sum())
     return bool(feas), nodes[:total].copy(), lens, cost.value, steps.value, used.value
 

@@ -207,3 +207,35 @@ def test_deposit_touches_route_arcs_only(oracle_mod):
         off += ln
     assert changed <= arcs and len(changed) > 0
     assert np.all(out >= tau)
+
+
+def test_cuda_ref_depot_rule_serves_everyone(oracle_mod):
+    """Reference-CUDA depot rule in the oracle: every customer served once,
+    and with roomy capacity the routes differ from the sequential rule's."""
+    import ctypes
+    O = oracle_mod
+    base = I.uniform_instance(150, 4, 905).unit_twin()
+    inst = I.Instance("roomy", base.x, base.y, base.demand, 4, 80)
+    n, K, k = inst.n, 4, 16
+    A, lut, thr = O.tables()
+    P = O.params()
+    cand = O.knn(inst.x, inst.y, k)
+    lvl = O.levels(inst.x, inst.y, cand, k, thr)
+    tau = np.full((n + 1) ** 2, P["q_tau0"], np.uint8)
+    w = O.weights(n, k, cand, lvl, tau, A, lut)
+    d2 = ((inst.x - inst.x[0]) ** 2 + (inst.y - inst.y[0]) ** 2).astype(np.float32)
+    lvl0 = np.array([O.lib().orc_level(float(v), thr.ctypes.data_as(ctypes.c_void_p), len(thr))
+                     for v in d2], np.uint16)
+    e_dep = int(round(16.0 * (1.0 - np.float64(np.float32(np.log(np.float32(1e-4)))) / np.log(2.0))))
+    rdep = O.depot_rel(n, k, cand, lvl, tau, A, lvl0, e_dep)
+    differs = 0
+    for a in range(24):
+        f, nodes, lens, cost, steps, used = O.construct_ant(
+            inst.x, inst.y, None, K, inst.capacity, k, cand, w, 5, 0, a, rule=1, rdep=rdep,
+            lut=lut)
+        assert f and sorted(nodes[nodes > 0]) == list(range(1, n + 1))
+        assert all(nodes[np.cumsum(lens) - 1] == 0) and lens.sum() == n + 2 * K
+        f0, n0, l0, *_ = O.construct_ant(inst.x, inst.y, None, K, inst.capacity, k, cand, w,
+                                         5, 0, a)
+        differs += int(not np.array_equal(lens, l0) or not np.array_equal(nodes, n0))
+    assert differs > 0

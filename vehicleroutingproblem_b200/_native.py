@@ -39,6 +39,7 @@ EXPORTED = [
     "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
     "aco_b200_batch_get", "aco_b200_batch_get_costs",
     "aco_b200_shard_packet_ints", "aco_b200_shard_construct", "aco_b200_shard_update",
+    "aco_b200_get_depot_tables",
     "aco_b200_prior_create", "aco_b200_prior_destroy", "aco_b200_prior_set_stream",
     "aco_b200_prior_init", "aco_b200_prior_set_params", "aco_b200_prior_get_params",
     "aco_b200_prior_load", "aco_b200_prior_save", "aco_b200_prior_set_dataset",
@@ -72,7 +73,7 @@ class Problem(C.Structure):
                 ("tau0", C.c_double), ("Q", C.c_double), ("seed", C.c_uint),
                 ("stagnation_epochs", C.c_int), ("fixed_epochs", C.c_int),
                 ("min_rel_improvement", C.c_double), ("timeout_seconds", C.c_double),
-                ("ant_base", C.c_int)]
+                ("ant_base", C.c_int), ("depot_rule", C.c_int)]
 
 
 class State(C.Structure):
@@ -136,6 +137,7 @@ def load():
         "aco_b200_batch_get_costs": [vp, vp, vp, vp],
         "aco_b200_shard_packet_ints": [vp], "aco_b200_shard_construct": [vp, vp],
         "aco_b200_shard_update": [vp, vp, i32],
+        "aco_b200_get_depot_tables": [vp, vp, vp, vp],
         "aco_b200_prior_create": [vp, i32], "aco_b200_prior_destroy": [vp],
         "aco_b200_prior_set_stream": [vp, vp], "aco_b200_prior_init": [vp, C.c_uint],
         "aco_b200_prior_set_params": [vp, vp, i32], "aco_b200_prior_get_params": [vp, vp, i32],
@@ -205,7 +207,7 @@ class Context:
               cand_k: int = 0, alpha=1.0, beta=2.0, rho=0.5, tau0=1.0, Q=1.0,
               seed: int = 1234, stagnation_epochs: int = 0, fixed_epochs: int = 0,
               min_rel_improvement: float = 1e-3, timeout_seconds: float = 0.0,
-              ant_base: int = 0):
+              ant_base: int = 0, depot_rule: int = 0):
         x = np.ascontiguousarray(x, np.float32)
         y = np.ascontiguousarray(y, np.float32)
         d = None if demand is None else np.ascontiguousarray(demand, np.int32)
@@ -215,7 +217,7 @@ class Context:
                     alpha=alpha, beta=beta, rho=rho, tau0=tau0, Q=Q, seed=seed & 0xffffffff,
                     stagnation_epochs=stagnation_epochs, fixed_epochs=fixed_epochs,
                     min_rel_improvement=min_rel_improvement, timeout_seconds=timeout_seconds,
-                    ant_base=ant_base)
+                    ant_base=ant_base, depot_rule=depot_rule)
         _check(self._lib.aco_b200_setup(self._h, C.byref(p)), "aco_b200_setup")
         n, K_, k, m = C.c_int(), C.c_int(), C.c_int(), C.c_int()
         _check(self._lib.aco_b200_get_dims(self._h, C.byref(n), C.byref(K_), C.byref(k),
@@ -297,6 +299,16 @@ class Context:
         w = np.zeros((self.n + 1) * self.k, np.uint32)
         _check(self._lib.aco_b200_get_weights(self._h, _p(w)), "aco_b200_get_weights")
         return w
+
+    def depot_tables(self):
+        """Reference-CUDA depot rule: (lvl0 [n+1], rdep [n+1] of the last
+        weights pass, e_dep)."""
+        lvl0 = np.zeros(self.n + 1, np.uint16)
+        rdep = np.zeros(self.n + 1, np.int32)
+        e = C.c_int()
+        _check(self._lib.aco_b200_get_depot_tables(self._h, _p(lvl0), _p(rdep), C.byref(e)),
+               "aco_b200_get_depot_tables")
+        return lvl0, rdep, e.value
 
     def construct(self, epoch: int, layout: int = LAYOUT_AUTO) -> None:
         _check(self._lib.aco_b200_construct(self._h, epoch, layout), "aco_b200_construct")

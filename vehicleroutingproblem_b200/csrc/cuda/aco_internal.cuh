@@ -32,6 +32,10 @@ constexpr int kStopFixed = 2;
 constexpr int kStopTimeout = 4;
 constexpr int kStopRunLimit = 8;
 
+// Depot rules of the construction (InstanceView::depot_rule).
+constexpr int kDepotRuleSeq = 0;      // src/seq/aco_sequential.c:616-681
+constexpr int kDepotRuleCudaRef = 1;  // stochastic close, aco_cuda_kernels.cu:487-520
+
 // Device error bits (DevState::error).
 constexpr int kErrStageTimeout = 1;
 
@@ -99,6 +103,7 @@ struct InstanceView {
   int max_demand;          // largest customer demand
   int route_stride;        // n + 2K
   int ant_base;            // global id of local ant 0 (colony split over devices)
+  int depot_rule;          // kDepotRuleSeq or kDepotRuleCudaRef
   const float2 *coords;    // [n+1]
   const int *demand;       // [n+1]
   const uint16_t *cand;    // [(n+1) k]
@@ -122,6 +127,11 @@ struct EpochTables {
   uint8_t *rel;            // [(n+1) k] weight levels below the row maximum
   const int32_t *A;        // [256]
   const uint32_t *lut;     // [256]
+  // Reference-CUDA depot rule only (else null): per row, the depot-close
+  // weight's level below the row maximum, rdep[i] = emax_i - (e_dep - lvl0[i]).
+  int32_t *rdep;           // [(n+1)]
+  const uint16_t *lvl0;    // [(n+1)] eta level of d(i,0)^2
+  int e_dep;               // level of the depot factor 2 / tau_min^alpha
 };
 
 struct PheromoneView {
@@ -155,6 +165,8 @@ cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
                                 unsigned int *counter, int grid,
                                 cudaStream_t s);
 cudaError_t launch_set_run_limit(DevState *st, int limit, cudaStream_t s);
+cudaError_t launch_depot_levels(const float2 *coords, int n, const float *thr, int J,
+                                uint16_t *lvl0, cudaStream_t s);
 int shard_packet_size(int n, int K);
 cudaError_t launch_shard_pack(const InstanceView &iv, const AntBuffers &ab, DevState *st,
                               int *send, cudaStream_t s);

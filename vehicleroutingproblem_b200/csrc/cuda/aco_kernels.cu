@@ -63,6 +63,20 @@ cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
   return cudaGetLastError();
 }
 
+// eta level of d(i,0)^2 for every node (reference-CUDA depot rule).
+__global__ void k_depot_levels(const float2 *__restrict__ coords, int n,
+                               const float *__restrict__ thr, int J, uint16_t *lvl0) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > n) return;
+  lvl0[i] = (uint16_t)level_of(dist2f(coords[i], coords[0]), thr, J);
+}
+
+cudaError_t launch_depot_levels(const float2 *coords, int n, const float *thr, int J,
+                                uint16_t *lvl0, cudaStream_t s) {
+  k_depot_levels<<<(n + 1 + 255) / 256, 256, 0, s>>>(coords, n, thr, J, lvl0);
+  return cudaGetLastError();
+}
+
 // ===========================================================================
 // Byte fill (pheromone initialisation, kernel_init_tau :131-136)
 // ===========================================================================
@@ -123,6 +137,8 @@ __global__ void __launch_bounds__(256) k_weights(InstanceView iv,
       }
     }
     int emax = __reduce_max_sync(kFull, e);
+    if (et.rdep && lane == 0)
+      et.rdep[i] = (emax == INT_MIN) ? 0 : emax - (et.e_dep - (int)et.lvl0[i]);
     if (lane < k) {
       uint32_t w = 0u;
       uint8_t rel = (uint8_t)kRelMax;
@@ -312,13 +328,30 @@ __device__ __forceinline__ double route_cost(const Tables<L, UNIT> &tb,
   return acc;
 }
 
+// Depot-close weight of the reference-CUDA rule on the scale of the row's
+// candidate weights: 2^23 2^(-r/16) for r = rdep (may be negative, i.e. above
+// the row maximum), exact in FP64 as LUT[r mod 16] 2^(-floor(r/16)); 0 from
+// r = 255 on, like the candidate weights.
+__device__ __forceinline__ double depot_weight(int r, const uint32_t *lut) {
+  if (r >= kRelMax) return 0.0;
+  const int q = (r >= 0) ? (r / 16) : -((-r + 15) / 16);
+  return ldexp((double)__ldg(lut + (r - 16 * q)), -q);
+}
+
 // One ant, one warp.  Rules of build_ant_solution
 // (src/seq/aco_sequential.c:616-681) with the demand extension:
 //   vehicle v extends while remaining > 0, remaining demand > (K-v-1) Q and
 //   load < Q; the next customer is drawn by roulette over the eligible
 //   candidates (unvisited, load + d <= Q), else the nearest eligible one;
 //   customers left over are added by the backward repair pass.
-template <int L, bool UNIT, int V>
+// CREF (reference-CUDA depot rule, kernel_construct_solutions,
+// src/cuda/aco_cuda_kernels.cu:487-520): vehicle v extends while customers
+// remain and load < Q; once the remaining demand fits the later vehicles
+// (<= (K-v-1) Q) the route may close: at the depot it closes at once (the
+// reference's 2 (1/(0+eps))^beta dwarfs every candidate), with no eligible
+// candidate it closes, and after a roulette draw a second draw u closes it
+// when u (denom + w_depot) >= denom, w_depot = depot_weight(rdep[cur]).
+template <int L, bool UNIT, int V, bool CREF>
 __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
                           Visited<V> &vis, uint32_t *dbuf, int ant,
                           uint32_t epoch, int lane) {
@@ -361,7 +394,10 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
     }
     if (!UNIT) dc = tb.demand(c);
     // Every demand is >= 1, so rem_dem > future >= 0 implies remaining > 0.
-    while (rem_dem > future && load < cap) {
+    const int limit = CREF ? 0 : future;
+    while (rem_dem > limit && load < cap) {
+      const bool may_close = CREF && rem_dem <= future;
+      if (CREF && may_close && cur == 0) break;
       bool ok = !vis.test(c);
       // Demands only bind when the room left is below the largest demand;
       // until then the speculative demand load stays off the step's chain.
@@ -391,6 +427,20 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       const int src = msk ? __ffs(msk) - 1 : 0;
       int next = __shfl_sync(kFull, c, src);
       int dn = UNIT ? 1 : __shfl_sync(kFull, dc, src);
+      bool drawn = false;  // draws of this step already accounted
+      if (CREF && may_close) {
+        if (denom == 0u) break;
+        d += 1u;  // the roulette draw is spent
+        if ((d & 127u) == 0u) draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
+        const uint32_t r2 = dbuf[d & 127u];
+        d += 1u;  // and the close draw
+        if ((d & 127u) == 0u) draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
+        r_next = dbuf[d & 127u];
+        drawn = true;
+        const double wd = depot_weight(a.et.rdep[cur], a.et.lut);
+        if (__dmul_rn((double)r2, __dadd_rn((double)denom, wd)) >= (double)denom * 16777216.0)
+          break;
+      }
       if (denom == 0u) {
         next = nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), room, tight, lane);
         if (next <= 0) break;
@@ -416,10 +466,12 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       tight = !UNIT && room < max_dem;
       cur = next;
       // A draw is consumed only by a roulette selection (denom > 0).
-      d += (denom != 0u) ? 1u : 0u;
-      if ((d & 127u) == 0u && denom != 0u)
-        draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
-      r_next = dbuf[d & 127u];
+      if (!CREF || !drawn) {
+        d += (denom != 0u) ? 1u : 0u;
+        if ((d & 127u) == 0u && denom != 0u)
+          draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
+        r_next = dbuf[d & 127u];
+      }
     }
     if (lane == 0) {
       route[pos] = 0;
@@ -492,7 +544,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
   }
 }
 
-template <int L, bool UNIT, int V>
+template <int L, bool UNIT, int V, bool CREF>
 __global__ void __launch_bounds__(512, 1) k_construct(ConstructArgs a) {
   if (a.st && *(volatile int *)&a.st->skip) return;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -560,7 +612,7 @@ __global__ void __launch_bounds__(512, 1) k_construct(ConstructArgs a) {
   const int ant = blockIdx.x * pl.wpb + warp;
   if (ant >= iv.m) return;
   const uint32_t epoch = a.use_state_epoch ? (uint32_t)a.st->epoch : a.epoch;
-  build_ant<L, UNIT, V>(a, tb, vis, dbuf, ant, epoch, lane);
+  build_ant<L, UNIT, V, CREF>(a, tb, vis, dbuf, ant, epoch, lane);
 }
 
 static int g_max_smem = 0;
@@ -626,9 +678,13 @@ SmemPlan plan_construct(const InstanceView &iv, int layout, int num_sms,
 
 template <int L, bool UNIT, int V>
 static cudaError_t configure_t() {
-  return cudaFuncSetAttribute(k_construct<L, UNIT, V>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              construct_max_smem());
+  cudaError_t e = cudaFuncSetAttribute(k_construct<L, UNIT, V, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       construct_max_smem());
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_construct<L, UNIT, V, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, construct_max_smem());
+  return e;
 }
 
 template <int L, bool UNIT>
@@ -651,16 +707,25 @@ cudaError_t prepare_construct_kernels() {
   return e;
 }
 
-template <int L, bool UNIT>
-static cudaError_t launch_construct_lu(const ConstructArgs &a, cudaStream_t s) {
+template <int L, bool UNIT, bool CREF>
+static cudaError_t launch_construct_luc(const ConstructArgs &a, cudaStream_t s) {
   const int grid = (a.iv.m + a.plan.wpb - 1) / a.plan.wpb;
   const int threads = a.plan.wpb * 32;
   switch (a.plan.vreg) {
-    case 1: k_construct<L, UNIT, 1><<<grid, threads, a.plan.total, s>>>(a); break;
-    case 2: k_construct<L, UNIT, 2><<<grid, threads, a.plan.total, s>>>(a); break;
-    default: k_construct<L, UNIT, 0><<<grid, threads, a.plan.total, s>>>(a); break;
+    case 1: k_construct<L, UNIT, 1, CREF><<<grid, threads, a.plan.total, s>>>(a); break;
+    case 2: k_construct<L, UNIT, 2, CREF><<<grid, threads, a.plan.total, s>>>(a); break;
+    default: k_construct<L, UNIT, 0, CREF><<<grid, threads, a.plan.total, s>>>(a); break;
   }
   return cudaGetLastError();
+}
+
+template <int L, bool UNIT>
+static cudaError_t launch_construct_lu(const ConstructArgs &a, cudaStream_t s) {
+  if (a.iv.depot_rule == kDepotRuleCudaRef) {
+    if (!a.et.rdep) return cudaErrorInvalidValue;
+    return launch_construct_luc<L, UNIT, true>(a, s);
+  }
+  return launch_construct_luc<L, UNIT, false>(a, s);
 }
 
 cudaError_t launch_construct(const InstanceView &iv, const EpochTables &et,

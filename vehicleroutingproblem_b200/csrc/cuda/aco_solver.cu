@@ -86,6 +86,8 @@ struct aco_b200_ctx {
   int *d_gbest_nodes = nullptr, *d_gbest_lens = nullptr;
   int *d_tmp_nodes = nullptr, *d_tmp_lens = nullptr;
   int *d_iter_nodes = nullptr, *d_iter_lens = nullptr;  // exchanged iteration best
+  int32_t *d_rdep = nullptr;  // depot rule 1: depot-close levels per row
+  uint16_t *d_lvl0 = nullptr; // depot rule 1: eta level of d(i,0)^2
   unsigned int *d_counter = nullptr;
 
   // host mirrors
@@ -114,7 +116,7 @@ void aco_b200_ctx::free_buffers() {
                   d_w, d_rel, ab.routes, ab.lens, ab.cost, ab.feasible, ab.steps,
                   ab.draws, ab.loads, ab.rep, ab.repc, d_state, d_log,
                   d_gbest_nodes, d_gbest_lens, d_tmp_nodes, d_tmp_lens, d_iter_nodes,
-                  d_iter_lens, d_counter};
+                  d_iter_lens, d_counter, d_rdep, d_lvl0};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d_coords = nullptr; d_demand = nullptr; d_cand = d_lvl = nullptr; d_thr = nullptr;
@@ -122,6 +124,7 @@ void aco_b200_ctx::free_buffers() {
   ab = AntBuffers{};
   d_state = nullptr; d_log = nullptr; d_gbest_nodes = d_gbest_lens = nullptr;
   d_tmp_nodes = d_tmp_lens = nullptr; d_iter_nodes = d_iter_lens = nullptr;
+  d_rdep = nullptr; d_lvl0 = nullptr;
   d_counter = nullptr;
   ready = false;
 }
@@ -316,6 +319,10 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   if (k > n) k = n;
   int m = p->ants > 0 ? p->ants : 256;
   if ((long long)m * (n + 2LL * p->K) > (1LL << 31)) return ACO_ERR_INVALID_INPUT;
+  if (p->depot_rule != kDepotRuleSeq && p->depot_rule != kDepotRuleCudaRef) {
+    fprintf(stderr, "aco_b200: invalid depot_rule=%d (0 or 1)\n", p->depot_rule);
+    return ACO_ERR_INVALID_INPUT;
+  }
   if (p->ant_base < 0 || (long long)p->ant_base + m > 0x7fffffffLL) {
     fprintf(stderr, "aco_b200: invalid ant_base=%d\n", p->ant_base);
     return ACO_ERR_INVALID_INPUT;
@@ -365,6 +372,10 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   TRY_ALLOC(dalloc(&ctx->d_tmp_lens, (size_t)p->K));
   TRY_ALLOC(dalloc(&ctx->d_iter_nodes, (size_t)R));
   TRY_ALLOC(dalloc(&ctx->d_iter_lens, (size_t)p->K));
+  if (p->depot_rule == kDepotRuleCudaRef) {
+    TRY_ALLOC(dalloc(&ctx->d_rdep, rows));
+    TRY_ALLOC(dalloc(&ctx->d_lvl0, rows));
+  }
   TRY_ALLOC(dalloc(&ctx->d_counter, 1));
 
   std::vector<float2> xy(rows);
@@ -390,6 +401,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   iv.max_demand = max_demand;
   iv.route_stride = R;
   iv.ant_base = p->ant_base;
+  iv.depot_rule = p->depot_rule;
   iv.coords = ctx->d_coords;
   iv.demand = ctx->d_demand;
   iv.cand = ctx->d_cand;
@@ -406,6 +418,11 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   ctx->et.rel = ctx->d_rel;
   ctx->et.A = ctx->d_A;
   ctx->et.lut = ctx->d_lut;
+  ctx->et.rdep = ctx->d_rdep;
+  ctx->et.lvl0 = ctx->d_lvl0;
+  // Level of the reference's depot factor 2 relative to the candidates'
+  // tau_min^alpha scale: 16 (1 - alpha log2 tau_min).
+  ctx->et.e_dep = (int)llround(16.0 * (1.0 - p->alpha * (double)ctx->log_min / log(2.0)));
   ctx->plan = plan_construct(iv, -1, ctx->num_sms, ctx->max_smem);
   {
     unsigned long long nvec = tau_total / 16;
@@ -417,6 +434,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
 
   TRY(launch_knn_levels(ctx->d_coords, n, k, ctx->d_thr, kThresholds, ctx->d_cand, ctx->d_lvl, s));
   TRY(launch_fill_u8(ctx->d_tau, tau_total, ctx->q_tau0, s));
+  if (ctx->d_lvl0) TRY(launch_depot_levels(ctx->d_coords, n, ctx->d_thr, kThresholds, ctx->d_lvl0, s));
 
   DevState st = {};
   st.global_best = DBL_MAX;
@@ -528,6 +546,17 @@ int aco_b200_enqueue_epochs(aco_b200_ctx *ctx, int epochs) {
     left -= kChunkEpochs;
   }
   for (int i = 0; i < left; ++i) TRY(cudaGraphLaunch(ctx->graph_one, s));
+  return ACO_OK;
+}
+
+int aco_b200_get_depot_tables(aco_b200_ctx *ctx, uint16_t *lvl0, int32_t *rdep, int *e_dep) {
+  if (!ctx || !ctx->ready || !ctx->d_rdep) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(ctx->device);
+  TRY(cudaStreamSynchronize(ctx->stream));
+  const size_t rows = (size_t)ctx->n + 1;
+  if (lvl0) TRY(cudaMemcpy(lvl0, ctx->d_lvl0, rows * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+  if (rdep) TRY(cudaMemcpy(rdep, ctx->d_rdep, rows * sizeof(int32_t), cudaMemcpyDeviceToHost));
+  if (e_dep) *e_dep = ctx->et.e_dep;
   return ACO_OK;
 }
 
@@ -861,6 +890,11 @@ static AcoStatus solve_impl(int n, int K, long long capacity, int m,
   prob.fixed_epochs = cfg.fixed_epochs;
   prob.min_rel_improvement = cfg.min_rel_improvement;
   prob.timeout_seconds = cfg.timeout_seconds;
+  // ACO_CUDA_DEPOT_RULE: seq (default) or cuda_ref.
+  const char *rule = getenv("ACO_CUDA_DEPOT_RULE");
+  if (rule && strcmp(rule, "cuda_ref") == 0) prob.depot_rule = kDepotRuleCudaRef;
+  else if (rule && *rule && strcmp(rule, "seq") != 0)
+    fprintf(stderr, "[cuda] ACO_CUDA_DEPOT_RULE=%s not recognised (seq|cuda_ref): seq\n", rule);
 
   aco_b200_ctx *ctx = nullptr;
   int rc = aco_b200_create(&ctx, 0);

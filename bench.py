@@ -239,7 +239,7 @@ def cpu_baseline_batched(insts, target_s=15.0):
                        f"to the batch by n+K, OMP_NUM_THREADS={threads}")}
 
 
-def cli_epoch_rate(binary, inst, ants, seconds=CLI_SECONDS):
+def cli_epoch_rate(binary, inst, ants, seconds=CLI_SECONDS, extra_env=None):
     """Epoch rate of a solver binary with the reference CLI contract
     (`<vrp> <K> <m> <seed>`, ACO_SOLVER_* env) on the unit-demand twin, from
     its last `[progress][cuda] epoca=E | ... tempo_trascorso=S s` line under
@@ -250,6 +250,7 @@ def cli_epoch_rate(binary, inst, ants, seconds=CLI_SECONDS):
     env = dict(os.environ, ACO_SOLVER_TIMEOUT_SECONDS=str(seconds),
                ACO_SOLVER_STAGNATION_EPOCHS="0", ACO_SOLVER_PROGRESS_INTERVAL_SECONDS="0")
     env.pop("ACO_SOLVER_FIXED_EPOCHS", None)
+    env.update(extra_env or {})
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, twin.name + ".vrp")
         I.write_vrp(twin, path)
@@ -421,6 +422,10 @@ def run_single(args, rank, world, local, torch, dist, _native):
             # comparable with the reference arm's reference_cuda_same_gpu.
             try:
                 line["cli_same_contract"] = cli_epoch_rate(OUR_CLI, inst, m)
+                # the reference CUDA kernel's depot-close rule, for a cost
+                # comparison with reference_cuda_same_gpu
+                line["cli_same_contract_cuda_ref_rule"] = cli_epoch_rate(
+                    OUR_CLI, inst, m, extra_env={"ACO_CUDA_DEPOT_RULE": "cuda_ref"})
             except Exception as exc:  # reported, not fatal
                 line["cli_same_contract"] = {"error": str(exc)[:200]}
     ctx.close()

@@ -398,3 +398,24 @@ def test_stop_rules_and_determinism():
         assert st.epochs == 21 and not st.stopped
         st = ctx.run(5)
         assert st.epochs == 26
+
+
+def test_setup_reuse_matches_fresh_contexts():
+    """A context set up again with the same sizes keeps its buffers and, when
+    the captured arguments match, its epoch graphs; every solve must equal a
+    fresh context's (seed, instance and parameters changed in between)."""
+    a = I.uniform_instance(180, 4, 620)
+    b = I.uniform_instance(180, 4, 621)  # same sizes, other coordinates and demands
+    runs = [(a, 5, 0.5), (a, 6, 0.5), (b, 6, 0.5), (a, 7, 0.3), (a, 5, 0.5)]
+    with make_ctx(a, 24, 40, seed=5) as reused:
+        for inst, seed, rho in runs:
+            reused.setup_instance(inst, ants=40, cand_k=24, seed=seed, rho=rho)
+            st = reused.run(21)
+            with make_ctx(inst, 24, 40, seed=seed, rho=rho) as fresh:
+                sf = fresh.run(21)
+                assert (st.epochs, st.global_best, st.total_steps, st.iter_since_best) == \
+                    (sf.epochs, sf.global_best, sf.total_steps, sf.iter_since_best)
+                assert np.array_equal(reused.tau(), fresh.tau())
+                bn, bl, bc = reused.best()
+                fn, fl, fc = fresh.best()
+                assert bc == fc and np.array_equal(bn, fn) and np.array_equal(bl, fl)

@@ -81,7 +81,7 @@ struct DevState {
   double min_rel;
   unsigned long long timeout_ns;
   float Qs;                // Q * 100 (src/cuda/aco_cuda.cu:228)
-  int pad0;
+  uint32_t seed;           // draw seed of the graph-launched epochs
 };
 
 // Byte offsets of the construct kernel's dynamic shared memory.

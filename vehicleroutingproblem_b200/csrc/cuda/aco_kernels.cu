@@ -354,7 +354,7 @@ __device__ __forceinline__ double depot_weight(int r, const uint32_t *lut) {
 template <int L, bool UNIT, int V, bool CREF>
 __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
                           Visited<V> &vis, uint32_t *dbuf, int ant,
-                          uint32_t epoch, int lane) {
+                          uint32_t epoch, uint32_t seed, int lane) {
   const InstanceView &iv = a.iv;
   const int k = iv.k, K = iv.K, R = iv.route_stride;
   const int cap = (int)iv.cap;
@@ -367,7 +367,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
   // split over several devices).
   const uint32_t gant = (uint32_t)(ant + iv.ant_base);
   uint32_t d = 0;
-  draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
+  draw_refill(dbuf, d, seed, epoch, gant, a.stream, lane);
   uint32_t r_next = dbuf[0];
 
   int remaining = iv.n;
@@ -431,10 +431,10 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       if (CREF && may_close) {
         if (denom == 0u) break;
         d += 1u;  // the roulette draw is spent
-        if ((d & 127u) == 0u) draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
+        if ((d & 127u) == 0u) draw_refill(dbuf, d, seed, epoch, gant, a.stream, lane);
         const uint32_t r2 = dbuf[d & 127u];
         d += 1u;  // and the close draw
-        if ((d & 127u) == 0u) draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
+        if ((d & 127u) == 0u) draw_refill(dbuf, d, seed, epoch, gant, a.stream, lane);
         r_next = dbuf[d & 127u];
         drawn = true;
         const double wd = depot_weight(a.et.rdep[cur], a.et.lut);
@@ -469,7 +469,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       if (!CREF || !drawn) {
         d += (denom != 0u) ? 1u : 0u;
         if ((d & 127u) == 0u && denom != 0u)
-          draw_refill(dbuf, d, a.seed, epoch, gant, a.stream, lane);
+          draw_refill(dbuf, d, seed, epoch, gant, a.stream, lane);
         r_next = dbuf[d & 127u];
       }
     }
@@ -611,8 +611,11 @@ __global__ void __launch_bounds__(512, 1) k_construct(ConstructArgs a) {
 
   const int ant = blockIdx.x * pl.wpb + warp;
   if (ant >= iv.m) return;
+  // Graph replays read the epoch number and the seed from the device state,
+  // so one captured graph serves every solve of a context.
   const uint32_t epoch = a.use_state_epoch ? (uint32_t)a.st->epoch : a.epoch;
-  build_ant<L, UNIT, V, CREF>(a, tb, vis, dbuf, ant, epoch, lane);
+  const uint32_t seed = a.use_state_epoch ? a.st->seed : a.seed;
+  build_ant<L, UNIT, V, CREF>(a, tb, vis, dbuf, ant, epoch, seed, lane);
 }
 
 static int g_max_smem = 0;

@@ -103,10 +103,34 @@ struct aco_b200_ctx {
   cudaGraphExec_t graph_chunk = nullptr;
   cudaGraphExec_t graph_one = nullptr;
   bool run_limit_off = false;  // device run limit known to be disabled
+  int depot_rule = 0;
+  // Kernel arguments the graphs were captured with: a set-up that leaves
+  // them unchanged (same sizes, parameters and buffers) keeps the graphs.
+  unsigned char graph_key[sizeof(InstanceView) + sizeof(PheromoneView) + sizeof(EpochTables) +
+                          sizeof(AntBuffers) + sizeof(SmemPlan) + 8 * sizeof(void *)] = {};
+  void make_graph_key(unsigned char *key) const;
 
   void free_buffers();
   ~aco_b200_ctx();
 };
+
+void aco_b200_ctx::make_graph_key(unsigned char *key) const {
+  size_t o = 0;
+  auto put = [&](const void *p, size_t b) {
+    memcpy(key + o, p, b);
+    o += b;
+  };
+  put(&iv, sizeof(iv));
+  put(&pv, sizeof(pv));
+  put(&et, sizeof(et));
+  put(&ab, sizeof(ab));
+  put(&plan, sizeof(plan));
+  const void *ptrs[8] = {d_state, d_log, d_gbest_nodes, d_gbest_lens, d_counter, nullptr,
+                         nullptr, nullptr};
+  const long long grid = evap_grid;
+  memcpy((void *)&ptrs[5], &grid, sizeof(grid));
+  put(ptrs, sizeof(ptrs));
+}
 
 void aco_b200_ctx::free_buffers() {
   if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
@@ -329,7 +353,13 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   }
 
   cudaSetDevice(ctx->device);
-  ctx->free_buffers();
+  // Same sizes as the last set-up: the device buffers are reused (no
+  // allocation), and the graphs too when their captured arguments match.
+  const bool reuse = ctx->ready && ctx->n == n && ctx->K == p->K && ctx->k == k &&
+                     ctx->m == m && ctx->depot_rule == p->depot_rule;
+  if (!reuse) ctx->free_buffers();
+  ctx->ready = false;
+  ctx->depot_rule = p->depot_rule;
   ctx->n = n;
   ctx->K = p->K;
   ctx->k = k;
@@ -345,38 +375,40 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   const size_t rows = (size_t)n + 1;
   const int R = n + 2 * p->K;
   const unsigned long long tau_total = (unsigned long long)rows * rows;
-  TRY_ALLOC(dalloc(&ctx->d_coords, rows));
-  TRY_ALLOC(dalloc(&ctx->d_demand, rows));
-  TRY_ALLOC(dalloc(&ctx->d_cand, rows * k));
-  TRY_ALLOC(dalloc(&ctx->d_lvl, rows * k));
-  TRY_ALLOC(dalloc(&ctx->d_thr, (size_t)kThresholds));
-  TRY_ALLOC(dalloc(&ctx->d_A, 256));
-  TRY_ALLOC(dalloc(&ctx->d_lut, 256));
-  TRY_ALLOC(dalloc(&ctx->d_tau, (size_t)tau_total));
-  TRY_ALLOC(dalloc(&ctx->d_w, rows * k));
-  TRY_ALLOC(dalloc(&ctx->d_rel, rows * k));
-  TRY_ALLOC(dalloc(&ctx->ab.routes, (size_t)m * R));
-  TRY_ALLOC(dalloc(&ctx->ab.lens, (size_t)m * p->K));
-  TRY_ALLOC(dalloc(&ctx->ab.cost, (size_t)m));
-  TRY_ALLOC(dalloc(&ctx->ab.feasible, (size_t)m));
-  TRY_ALLOC(dalloc(&ctx->ab.steps, (size_t)m));
-  TRY_ALLOC(dalloc(&ctx->ab.draws, (size_t)m));
-  TRY_ALLOC(dalloc(&ctx->ab.loads, (size_t)m * p->K));
-  TRY_ALLOC(dalloc(&ctx->ab.rep, (size_t)m * n));
-  TRY_ALLOC(dalloc(&ctx->ab.repc, (size_t)m * p->K));
-  TRY_ALLOC(dalloc(&ctx->d_state, 1));
-  TRY_ALLOC(dalloc(&ctx->d_log, (size_t)kLogCap));
-  TRY_ALLOC(dalloc(&ctx->d_gbest_nodes, (size_t)R));
-  TRY_ALLOC(dalloc(&ctx->d_gbest_lens, (size_t)p->K));
-  TRY_ALLOC(dalloc(&ctx->d_tmp_nodes, (size_t)R));
-  TRY_ALLOC(dalloc(&ctx->d_tmp_lens, (size_t)p->K));
-  TRY_ALLOC(dalloc(&ctx->d_iter_nodes, (size_t)R));
-  TRY_ALLOC(dalloc(&ctx->d_iter_lens, (size_t)p->K));
-  if (p->depot_rule == kDepotRuleCudaRef) {
-    TRY_ALLOC(dalloc(&ctx->d_rdep, rows));
-    TRY_ALLOC(dalloc(&ctx->d_lvl0, rows));
+  if (!reuse) {
+    TRY_ALLOC(dalloc(&ctx->d_coords, rows));
+    TRY_ALLOC(dalloc(&ctx->d_demand, rows));
+    TRY_ALLOC(dalloc(&ctx->d_cand, rows * k));
+    TRY_ALLOC(dalloc(&ctx->d_lvl, rows * k));
+    TRY_ALLOC(dalloc(&ctx->d_thr, (size_t)kThresholds));
+    TRY_ALLOC(dalloc(&ctx->d_A, 256));
+    TRY_ALLOC(dalloc(&ctx->d_lut, 256));
+    TRY_ALLOC(dalloc(&ctx->d_tau, (size_t)tau_total));
+    TRY_ALLOC(dalloc(&ctx->d_w, rows * k));
+    TRY_ALLOC(dalloc(&ctx->d_rel, rows * k));
+    TRY_ALLOC(dalloc(&ctx->ab.routes, (size_t)m * R));
+    TRY_ALLOC(dalloc(&ctx->ab.lens, (size_t)m * p->K));
+    TRY_ALLOC(dalloc(&ctx->ab.cost, (size_t)m));
+    TRY_ALLOC(dalloc(&ctx->ab.feasible, (size_t)m));
+    TRY_ALLOC(dalloc(&ctx->ab.steps, (size_t)m));
+    TRY_ALLOC(dalloc(&ctx->ab.draws, (size_t)m));
+    TRY_ALLOC(dalloc(&ctx->ab.loads, (size_t)m * p->K));
+    TRY_ALLOC(dalloc(&ctx->ab.rep, (size_t)m * n));
+    TRY_ALLOC(dalloc(&ctx->ab.repc, (size_t)m * p->K));
+    TRY_ALLOC(dalloc(&ctx->d_state, 1));
+    TRY_ALLOC(dalloc(&ctx->d_log, (size_t)kLogCap));
+    TRY_ALLOC(dalloc(&ctx->d_gbest_nodes, (size_t)R));
+    TRY_ALLOC(dalloc(&ctx->d_gbest_lens, (size_t)p->K));
+    TRY_ALLOC(dalloc(&ctx->d_tmp_nodes, (size_t)R));
+    TRY_ALLOC(dalloc(&ctx->d_tmp_lens, (size_t)p->K));
+    TRY_ALLOC(dalloc(&ctx->d_iter_nodes, (size_t)R));
+    TRY_ALLOC(dalloc(&ctx->d_iter_lens, (size_t)p->K));
+    if (p->depot_rule == kDepotRuleCudaRef) {
+      TRY_ALLOC(dalloc(&ctx->d_rdep, rows));
+      TRY_ALLOC(dalloc(&ctx->d_lvl0, rows));
+    }
+    TRY_ALLOC(dalloc(&ctx->d_counter, 1));
   }
-  TRY_ALLOC(dalloc(&ctx->d_counter, 1));
 
   std::vector<float2> xy(rows);
   std::vector<int> dem(rows, 1);
@@ -384,6 +416,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   for (size_t i = 0; i < rows; ++i) xy[i] = make_float2(p->x[i], p->y[i]);
   if (p->demand) for (size_t i = 0; i < rows; ++i) dem[i] = p->demand[i];
   cudaStream_t s = ctx->stream;
+  if (reuse) TRY(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned int), s));
   TRY(cudaMemcpyAsync(ctx->d_coords, xy.data(), rows * sizeof(float2), cudaMemcpyHostToDevice, s));
   TRY(cudaMemcpyAsync(ctx->d_demand, dem.data(), rows * sizeof(int), cudaMemcpyHostToDevice, s));
   TRY(cudaMemcpyAsync(ctx->d_thr, ctx->thr.data(), kThresholds * sizeof(float), cudaMemcpyHostToDevice, s));
@@ -447,11 +480,21 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
                       ? (unsigned long long)(p->timeout_seconds * 1e9)
                       : 0ull;
   st.Qs = ctx->Qs;
+  st.seed = ctx->seed;
   *ctx->h_state = st;
   TRY(cudaMemcpyAsync(ctx->d_state, ctx->h_state, sizeof(DevState), cudaMemcpyHostToDevice, s));
   TRY(cudaStreamSynchronize(s));
   ctx->log_read = 0;
   ctx->run_limit_off = true;  // fresh state: run_limit = 0
+  unsigned char key[sizeof(ctx->graph_key)];
+  memset(key, 0, sizeof(key));
+  ctx->make_graph_key(key);
+  if (memcmp(key, ctx->graph_key, sizeof(key)) != 0) {
+    if (ctx->graph_chunk) cudaGraphExecDestroy(ctx->graph_chunk);
+    if (ctx->graph_one) cudaGraphExecDestroy(ctx->graph_one);
+    ctx->graph_chunk = ctx->graph_one = nullptr;
+    memcpy(ctx->graph_key, key, sizeof(key));
+  }
   ctx->ready = true;
   return ACO_OK;
 }

@@ -82,7 +82,17 @@ struct DevState {
   unsigned long long timeout_ns;
   float Qs;                // Q * 100 (src/cuda/aco_cuda.cu:228)
   uint32_t seed;           // draw seed of the graph-launched epochs
+  int tau_sel;             // current pheromone buffer (0: tau, 1: tau_alt)
+  int pad1;
 };
+
+// Current pheromone buffer.  The graph-launched epochs keep two: while the
+// ants are built the evaporated matrix is written into the other buffer,
+// the deposits go there, and the buffers switch (only when an iteration
+// best exists, as the reference evaporates only then).
+__device__ __forceinline__ uint8_t *cur_tau(uint8_t *tau, uint8_t *tau_alt, const DevState *st) {
+  return (tau_alt && st && *(volatile const int *)&st->tau_sel) ? tau_alt : tau;
+}
 
 // Byte offsets of the construct kernel's dynamic shared memory.
 struct SmemPlan {
@@ -132,6 +142,7 @@ struct EpochTables {
   int32_t *rdep;           // [(n+1)]
   const uint16_t *lvl0;    // [(n+1)] eta level of d(i,0)^2
   int e_dep;               // level of the depot factor 2 / tau_min^alpha
+  uint8_t *tau_alt;        // second pheromone buffer (pipelined epochs), or null
 };
 
 struct PheromoneView {
@@ -162,9 +173,15 @@ cudaError_t launch_best(const InstanceView &iv, const AntBuffers &ab,
 cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
                                 const AntBuffers &ab, DevState *st,
                                 const int *gbest_nodes, const int *gbest_lens,
-                                unsigned int *counter, int grid,
+                                unsigned int *counter, int grid, uint8_t *tau_alt,
                                 cudaStream_t s);
 cudaError_t launch_set_run_limit(DevState *st, int limit, cudaStream_t s);
+cudaError_t launch_evaporate_to(const PheromoneView &pv, uint8_t *tau_alt, DevState *st,
+                                int grid, cudaStream_t s);
+cudaError_t launch_best_deposit(const InstanceView &iv, const AntBuffers &ab,
+                                const PheromoneView &pv, uint8_t *tau_alt, DevState *st,
+                                int *gbest_nodes, int *gbest_lens, EpochRec *log,
+                                cudaStream_t s);
 cudaError_t launch_depot_levels(const float2 *coords, int n, const float *thr, int J,
                                 uint16_t *lvl0, cudaStream_t s);
 int shard_packet_size(int n, int K);
@@ -178,7 +195,8 @@ cudaError_t launch_evap_deposit_iter(const InstanceView &iv, const PheromoneView
                                      const AntBuffers &ab, DevState *st,
                                      const int *iter_nodes, const int *iter_lens,
                                      const int *gbest_nodes, const int *gbest_lens,
-                                     unsigned int *counter, int grid, cudaStream_t s);
+                                     unsigned int *counter, int grid, uint8_t *tau_alt,
+                                     cudaStream_t s);
 int construct_max_smem();
 cudaError_t prepare_construct_kernels();
 SmemPlan plan_construct(const InstanceView &iv, int layout, int num_sms,

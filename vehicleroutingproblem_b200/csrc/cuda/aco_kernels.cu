@@ -125,6 +125,7 @@ __global__ void __launch_bounds__(256) k_weights(InstanceView iv,
   const int warps = gridDim.x * (blockDim.x >> 5);
   const int k = iv.k;
   const size_t stride = (size_t)iv.n + 1;
+  const uint8_t *tau = cur_tau(pv.tau, et.tau_alt, st);
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i <= iv.n;
        i += warps) {
     int c = 0;
@@ -132,7 +133,7 @@ __global__ void __launch_bounds__(256) k_weights(InstanceView iv,
     if (lane < k) {
       c = iv.cand[(size_t)i * k + lane];
       if (c > 0) {
-        uint8_t q = pv.tau[(size_t)i * stride + c];
+        uint8_t q = tau[(size_t)i * stride + c];
         e = __ldg(et.A + q) - (int)iv.lvl[(size_t)i * k + lane];
       }
     }
@@ -819,9 +820,19 @@ __device__ int epoch_bookkeeping(DevState *st, bool found, double bc, int ba,
   return improved;
 }
 
-__global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
-                                               DevState *st, int *gbest_nodes,
-                                               int *gbest_lens, EpochRec *log) {
+__device__ __forceinline__ uint32_t evap4(uint32_t x, uint32_t floor4,
+                                          uint32_t delta4) {
+  return __vsub4(__vmaxu4(x, floor4), delta4);
+}
+
+// DEPOSIT: the pipelined epoch -- the evaporated matrix already sits in the
+// other pheromone buffer; this block deposits the iteration best and the
+// global best there and makes it the current buffer.
+template <bool DEPOSIT>
+__global__ void __launch_bounds__(1024) k_best_t(InstanceView iv, AntBuffers ab,
+                                                 DevState *st, int *gbest_nodes,
+                                                 int *gbest_lens, EpochRec *log,
+                                                 PheromoneView pv, uint8_t *tau_alt) {
   if (*(volatile int *)&st->skip) return;
   __shared__ double s_cost[32];
   __shared__ int s_ant[32];
@@ -889,12 +900,85 @@ __global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
     for (int t = threadIdx.x; t < total; t += blockDim.x) gbest_nodes[t] = src[t];
     for (int v = threadIdx.x; v < iv.K; v += blockDim.x) gbest_lens[v] = sl[v];
   }
+  if (DEPOSIT) {
+    if (s_best == INT_MAX) return;  // no feasible ant: no evaporation, no deposit
+    __syncthreads();                // the global-best copy is complete
+    const bool sel = *(volatile int *)&st->tau_sel != 0;
+    PheromoneView pd = pv;
+    pd.tau = sel ? pv.tau : tau_alt;  // the evaporated copy
+    const size_t stride_n = (size_t)iv.n + 1;
+    extern __shared__ int s_off[];
+    int *offs = (iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
+    const float dep_i = *(volatile float *)&st->dep_iter;
+    const float dep_g = *(volatile float *)&st->dep_global;
+    deposit_solution(pd, stride_n, CompactNodes{ab.routes + (size_t)s_best * iv.route_stride},
+                     ab.lens + (size_t)s_best * iv.K, iv.K, dep_i, offs);
+    __syncthreads();
+    deposit_solution(pd, stride_n, CompactNodes{gbest_nodes}, gbest_lens, iv.K, dep_g, offs);
+    __syncthreads();
+    if (threadIdx.x == 0) st->tau_sel = sel ? 0 : 1;
+  }
 }
 
 cudaError_t launch_best(const InstanceView &iv, const AntBuffers &ab,
                         DevState *st, int *gbest_nodes, int *gbest_lens,
                         EpochRec *log, cudaStream_t s) {
-  k_best<<<1, 1024, 0, s>>>(iv, ab, st, gbest_nodes, gbest_lens, log);
+  k_best_t<false><<<1, 1024, 0, s>>>(iv, ab, st, gbest_nodes, gbest_lens, log, PheromoneView{},
+                                     nullptr);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_best_deposit(const InstanceView &iv, const AntBuffers &ab,
+                                const PheromoneView &pv, uint8_t *tau_alt, DevState *st,
+                                int *gbest_nodes, int *gbest_lens, EpochRec *log,
+                                cudaStream_t s) {
+  const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
+  k_best_t<true><<<1, 1024, smem, s>>>(iv, ab, st, gbest_nodes, gbest_lens, log, pv, tau_alt);
+  return cudaGetLastError();
+}
+
+// Evaporation of the current pheromone buffer into the other one, run beside
+// the construction (which reads only the weights): 16 bytes per thread,
+// max(q, q_min + delta) - delta.
+__global__ void __launch_bounds__(512) k_evaporate_to(PheromoneView pv, uint8_t *tau_alt,
+                                                      DevState *st) {
+  if (*(volatile int *)&st->skip) return;
+  const bool sel = *(volatile int *)&st->tau_sel != 0;
+  const uint8_t *src = sel ? tau_alt : pv.tau;
+  uint8_t *dst = sel ? pv.tau : tau_alt;
+  const int fl = (int)pv.q_min + (int)pv.delta;
+  const bool sat_all = fl > 255;
+  const uint32_t floor4 = 0x01010101u * (uint32_t)(sat_all ? 0 : fl);
+  const uint32_t delta4 = 0x01010101u * (uint32_t)pv.delta;
+  const uint32_t qmin4 = 0x01010101u * (uint32_t)pv.q_min;
+  const unsigned long long nvec = pv.total / 16;
+  const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+  uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+       i < nvec; i += stride) {
+    uint4 v = s4[i];
+    if (sat_all) {
+      v = make_uint4(qmin4, qmin4, qmin4, qmin4);
+    } else {
+      v.x = evap4(v.x, floor4, delta4);
+      v.y = evap4(v.y, floor4, delta4);
+      v.z = evap4(v.z, floor4, delta4);
+      v.w = evap4(v.w, floor4, delta4);
+    }
+    d4[i] = v;
+  }
+  if (blockIdx.x == 0) {
+    for (unsigned long long i = nvec * 16 + threadIdx.x; i < pv.total; i += blockDim.x) {
+      const uint8_t q = src[i];
+      dst[i] = ((int)q > fl) ? (uint8_t)(q - pv.delta) : pv.q_min;
+    }
+  }
+}
+
+cudaError_t launch_evaporate_to(const PheromoneView &pv, uint8_t *tau_alt, DevState *st,
+                                int grid, cudaStream_t s) {
+  k_evaporate_to<<<grid, 512, 0, s>>>(pv, tau_alt, st);
   return cudaGetLastError();
 }
 
@@ -913,11 +997,6 @@ cudaError_t launch_set_run_limit(DevState *st, int limit, cudaStream_t s) {
 // Evaporation + deposit
 // ===========================================================================
 
-__device__ __forceinline__ uint32_t evap4(uint32_t x, uint32_t floor4,
-                                          uint32_t delta4) {
-  return __vsub4(__vmaxu4(x, floor4), delta4);
-}
-
 struct EvapArgs {
   InstanceView iv;
   PheromoneView pv;
@@ -930,13 +1009,15 @@ struct EvapArgs {
   unsigned int *counter;
   int best_ant;          // used when st == nullptr
   float dep_iter, dep_global;
+  uint8_t *tau_alt;      // second pheromone buffer of the context, or null
 };
 
 __global__ void __launch_bounds__(512) k_evap_deposit(EvapArgs a) {
   if (a.st) {
     if (*(volatile int *)&a.st->skip || !*(volatile int *)&a.st->found) return;
   }
-  const PheromoneView &pv = a.pv;
+  PheromoneView pv = a.pv;  // in place, on the current buffer
+  pv.tau = cur_tau(a.pv.tau, a.tau_alt, a.st);
   // q > q_min + delta ? q - delta : q_min  ==  max(q, q_min + delta) - delta
   const int fl = (int)pv.q_min + (int)pv.delta;
   const bool sat_all = fl > 255;
@@ -997,7 +1078,7 @@ __global__ void __launch_bounds__(512) k_evap_deposit(EvapArgs a) {
 cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
                                 const AntBuffers &ab, DevState *st,
                                 const int *gbest_nodes, const int *gbest_lens,
-                                unsigned int *counter, int grid,
+                                unsigned int *counter, int grid, uint8_t *tau_alt,
                                 cudaStream_t s) {
   EvapArgs a;
   a.iv = iv;
@@ -1011,6 +1092,7 @@ cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
   a.counter = counter;
   a.best_ant = 0;
   a.dep_iter = a.dep_global = 0.0f;
+  a.tau_alt = tau_alt;
   const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
   k_evap_deposit<<<grid, 512, smem, s>>>(a);
   return cudaGetLastError();
@@ -1039,6 +1121,7 @@ cudaError_t launch_evap_deposit_explicit(const InstanceView &iv,
   a.best_ant = best_ant;
   a.dep_iter = dep_iter;
   a.dep_global = dep_global;
+  a.tau_alt = nullptr;  // the caller passes the current buffer
   const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
   k_evap_deposit<<<grid, 512, smem, s>>>(a);
   return cudaGetLastError();
@@ -1194,7 +1277,8 @@ cudaError_t launch_evap_deposit_iter(const InstanceView &iv, const PheromoneView
                                      const AntBuffers &ab, DevState *st,
                                      const int *iter_nodes, const int *iter_lens,
                                      const int *gbest_nodes, const int *gbest_lens,
-                                     unsigned int *counter, int grid, cudaStream_t s) {
+                                     unsigned int *counter, int grid, uint8_t *tau_alt,
+                                     cudaStream_t s) {
   EvapArgs a;
   a.iv = iv;
   a.pv = pv;
@@ -1207,6 +1291,7 @@ cudaError_t launch_evap_deposit_iter(const InstanceView &iv, const PheromoneView
   a.counter = counter;
   a.best_ant = 0;
   a.dep_iter = a.dep_global = 0.0f;
+  a.tau_alt = tau_alt;
   const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
   k_evap_deposit<<<grid, 512, smem, s>>>(a);
   return cudaGetLastError();

@@ -55,6 +55,8 @@ struct aco_b200_ctx {
   int max_smem = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  cudaStream_t side = nullptr;       // evaporation beside the construction
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool ready = false;
 
   // problem
@@ -78,6 +80,7 @@ struct aco_b200_ctx {
   int32_t *d_A = nullptr;
   uint32_t *d_lut = nullptr;
   uint8_t *d_tau = nullptr;
+  uint8_t *d_tau2 = nullptr;  // second pheromone buffer of the pipelined epochs
   uint32_t *d_w = nullptr;
   uint8_t *d_rel = nullptr;
   AntBuffers ab = {};
@@ -136,7 +139,7 @@ void aco_b200_ctx::free_buffers() {
   if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
   if (graph_one) cudaGraphExecDestroy(graph_one);
   graph_chunk = graph_one = nullptr;
-  void *ptrs[] = {d_coords, d_demand, d_cand, d_lvl, d_thr, d_A, d_lut, d_tau,
+  void *ptrs[] = {d_coords, d_demand, d_cand, d_lvl, d_thr, d_A, d_lut, d_tau, d_tau2,
                   d_w, d_rel, ab.routes, ab.lens, ab.cost, ab.feasible, ab.steps,
                   ab.draws, ab.loads, ab.rep, ab.repc, d_state, d_log,
                   d_gbest_nodes, d_gbest_lens, d_tmp_nodes, d_tmp_lens, d_iter_nodes,
@@ -144,7 +147,8 @@ void aco_b200_ctx::free_buffers() {
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d_coords = nullptr; d_demand = nullptr; d_cand = d_lvl = nullptr; d_thr = nullptr;
-  d_A = nullptr; d_lut = nullptr; d_tau = nullptr; d_w = nullptr; d_rel = nullptr;
+  d_A = nullptr; d_lut = nullptr; d_tau = nullptr; d_tau2 = nullptr; d_w = nullptr;
+  d_rel = nullptr;
   ab = AntBuffers{};
   d_state = nullptr; d_log = nullptr; d_gbest_nodes = d_gbest_lens = nullptr;
   d_tmp_nodes = d_tmp_lens = nullptr; d_iter_nodes = d_iter_lens = nullptr;
@@ -158,6 +162,9 @@ aco_b200_ctx::~aco_b200_ctx() {
   free_buffers();
   if (h_state) cudaFreeHost(h_state);
   if (own_stream && stream) cudaStreamDestroy(stream);
+  if (side) cudaStreamDestroy(side);
+  if (ev_fork) cudaEventDestroy(ev_fork);
+  if (ev_join) cudaEventDestroy(ev_join);
 }
 
 #define TRY(call)                                                        \
@@ -218,18 +225,24 @@ static int build_graph(aco_b200_ctx *ctx, int epochs, cudaGraphExec_t *out) {
   cudaGraph_t g = nullptr;
   TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t err = cudaSuccess;
+  // One epoch: weights, then the construction and (on the side stream) the
+  // evaporation into the other pheromone buffer, then iteration best, global
+  // best, stop rules and the deposits, which switch the buffers.
   for (int e = 0; e < epochs && err == cudaSuccess; ++e) {
     err = launch_weights(ctx->iv, ctx->pv, ctx->et, ctx->d_state, ctx->stream);
+    if (err == cudaSuccess) err = cudaEventRecord(ctx->ev_fork, ctx->stream);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0);
+    if (err == cudaSuccess)
+      err = launch_evaporate_to(ctx->pv, ctx->d_tau2, ctx->d_state, ctx->evap_grid, ctx->side);
     if (err == cudaSuccess)
       err = launch_construct(ctx->iv, ctx->et, ctx->ab, ctx->plan, ctx->d_state,
                              ctx->seed, 0, 0, 1, ctx->stream);
+    if (err == cudaSuccess) err = cudaEventRecord(ctx->ev_join, ctx->side);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(ctx->stream, ctx->ev_join, 0);
     if (err == cudaSuccess)
-      err = launch_best(ctx->iv, ctx->ab, ctx->d_state, ctx->d_gbest_nodes,
-                        ctx->d_gbest_lens, ctx->d_log, ctx->stream);
-    if (err == cudaSuccess)
-      err = launch_evap_deposit(ctx->iv, ctx->pv, ctx->ab, ctx->d_state,
-                                ctx->d_gbest_nodes, ctx->d_gbest_lens,
-                                ctx->d_counter, ctx->evap_grid, ctx->stream);
+      err = launch_best_deposit(ctx->iv, ctx->ab, ctx->pv, ctx->d_tau2, ctx->d_state,
+                                ctx->d_gbest_nodes, ctx->d_gbest_lens, ctx->d_log,
+                                ctx->stream);
   }
   cudaError_t end = cudaStreamEndCapture(ctx->stream, &g);
   if (err != cudaSuccess || end != cudaSuccess) {
@@ -281,6 +294,9 @@ int aco_b200_create(aco_b200_ctx **out, int device) {
     return ACO_ERR_BACKEND;
   }
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming) != cudaSuccess ||
       cudaMallocHost((void **)&ctx->h_state, sizeof(DevState)) != cudaSuccess) {
     delete ctx;
     return ACO_ERR_BACKEND;
@@ -384,6 +400,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
     TRY_ALLOC(dalloc(&ctx->d_A, 256));
     TRY_ALLOC(dalloc(&ctx->d_lut, 256));
     TRY_ALLOC(dalloc(&ctx->d_tau, (size_t)tau_total));
+    TRY_ALLOC(dalloc(&ctx->d_tau2, (size_t)tau_total));
     TRY_ALLOC(dalloc(&ctx->d_w, rows * k));
     TRY_ALLOC(dalloc(&ctx->d_rel, rows * k));
     TRY_ALLOC(dalloc(&ctx->ab.routes, (size_t)m * R));
@@ -452,6 +469,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   ctx->et.A = ctx->d_A;
   ctx->et.lut = ctx->d_lut;
   ctx->et.rdep = ctx->d_rdep;
+  ctx->et.tau_alt = ctx->d_tau2;
   ctx->et.lvl0 = ctx->d_lvl0;
   // Level of the reference's depot factor 2 relative to the candidates'
   // tau_min^alpha scale: 16 (1 - alpha log2 tau_min).
@@ -646,7 +664,7 @@ int aco_b200_shard_update(aco_b200_ctx *ctx, const int32_t *d_recv, int world) {
                           ctx->d_iter_lens, ctx->d_gbest_nodes, ctx->d_gbest_lens, ctx->d_log, s));
   TRY(launch_evap_deposit_iter(ctx->iv, ctx->pv, ctx->ab, ctx->d_state, ctx->d_iter_nodes,
                                ctx->d_iter_lens, ctx->d_gbest_nodes, ctx->d_gbest_lens,
-                               ctx->d_counter, ctx->evap_grid, s));
+                               ctx->d_counter, ctx->evap_grid, ctx->d_tau2, s));
   return ACO_OK;
 }
 
@@ -672,7 +690,8 @@ int aco_b200_profile_epochs(aco_b200_ctx *ctx, int epochs, float *kernel_ms) {
     if (err == cudaSuccess) err = cudaEventRecord(ev[3], s);
     if (err == cudaSuccess)
       err = launch_evap_deposit(ctx->iv, ctx->pv, ctx->ab, ctx->d_state, ctx->d_gbest_nodes,
-                                ctx->d_gbest_lens, ctx->d_counter, ctx->evap_grid, s);
+                                ctx->d_gbest_lens, ctx->d_counter, ctx->evap_grid,
+                                ctx->d_tau2, s);
     if (err == cudaSuccess) err = cudaEventRecord(ev[4], s);
     if (err == cudaSuccess) err = cudaEventSynchronize(ev[4]);
     for (int i = 0; i < 4 && err == cudaSuccess; ++i) {
@@ -728,10 +747,22 @@ int aco_b200_get_best(aco_b200_ctx *ctx, int *nodes, int *lens, double *cost) {
   return ctx->h_state->global_best < DBL_MAX ? ACO_OK : ACO_ERR_NO_SOLUTION;
 }
 
+// The context's current pheromone buffer (read from the device state).
+static int current_tau(aco_b200_ctx *ctx, uint8_t **out) {
+  TRY(cudaMemcpyAsync(ctx->h_state, ctx->d_state, sizeof(DevState), cudaMemcpyDeviceToHost,
+                      ctx->stream));
+  TRY(cudaStreamSynchronize(ctx->stream));
+  *out = ctx->h_state->tau_sel ? ctx->d_tau2 : ctx->d_tau;
+  return ACO_OK;
+}
+
 int aco_b200_get_tau(aco_b200_ctx *ctx, uint8_t *tau) {
   if (!ctx || !ctx->ready || !tau) return ACO_ERR_INVALID_INPUT;
   cudaSetDevice(ctx->device);
-  TRY(cudaMemcpyAsync(tau, ctx->d_tau, ctx->pv.total, cudaMemcpyDeviceToHost, ctx->stream));
+  uint8_t *cur = nullptr;
+  int rc = current_tau(ctx, &cur);
+  if (rc) return rc;
+  TRY(cudaMemcpyAsync(tau, cur, ctx->pv.total, cudaMemcpyDeviceToHost, ctx->stream));
   TRY(cudaStreamSynchronize(ctx->stream));
   return ACO_OK;
 }
@@ -739,7 +770,10 @@ int aco_b200_get_tau(aco_b200_ctx *ctx, uint8_t *tau) {
 int aco_b200_set_tau(aco_b200_ctx *ctx, const uint8_t *tau) {
   if (!ctx || !ctx->ready || !tau) return ACO_ERR_INVALID_INPUT;
   cudaSetDevice(ctx->device);
-  TRY(cudaMemcpyAsync(ctx->d_tau, tau, ctx->pv.total, cudaMemcpyHostToDevice, ctx->stream));
+  uint8_t *cur = nullptr;
+  int rc = current_tau(ctx, &cur);
+  if (rc) return rc;
+  TRY(cudaMemcpyAsync(cur, tau, ctx->pv.total, cudaMemcpyHostToDevice, ctx->stream));
   TRY(cudaStreamSynchronize(ctx->stream));
   return ACO_OK;
 }
@@ -770,7 +804,12 @@ int aco_b200_get_tables(aco_b200_ctx *ctx, int32_t *A, uint32_t *lut,
 int aco_b200_get_weights(aco_b200_ctx *ctx, uint32_t *w) {
   if (!ctx || !ctx->ready || !w) return ACO_ERR_INVALID_INPUT;
   cudaSetDevice(ctx->device);
-  TRY(launch_weights(ctx->iv, ctx->pv, ctx->et, nullptr, ctx->stream));
+  PheromoneView pv = ctx->pv;
+  EpochTables et = ctx->et;
+  int rc = current_tau(ctx, &pv.tau);
+  if (rc) return rc;
+  et.tau_alt = nullptr;
+  TRY(launch_weights(ctx->iv, pv, et, nullptr, ctx->stream));
   const size_t cnt = ((size_t)ctx->n + 1) * ctx->k;
   TRY(cudaMemcpyAsync(w, ctx->d_w, cnt * 4, cudaMemcpyDeviceToHost, ctx->stream));
   TRY(cudaStreamSynchronize(ctx->stream));
@@ -784,7 +823,12 @@ int aco_b200_construct(aco_b200_ctx *ctx, int epoch, int layout) {
   SmemPlan plan = (layout < 0) ? ctx->plan
                                : plan_construct(ctx->iv, layout, ctx->num_sms, ctx->max_smem);
   if ((int)plan.total > ctx->max_smem) return ACO_ERR_INVALID_INPUT;
-  TRY(launch_weights(ctx->iv, ctx->pv, ctx->et, nullptr, ctx->stream));
+  PheromoneView pv = ctx->pv;
+  EpochTables et = ctx->et;
+  int rc = current_tau(ctx, &pv.tau);
+  if (rc) return rc;
+  et.tau_alt = nullptr;
+  TRY(launch_weights(ctx->iv, pv, et, nullptr, ctx->stream));
   TRY(launch_construct(ctx->iv, ctx->et, ctx->ab, plan, nullptr, ctx->seed,
                        (uint32_t)epoch, 0, 0, ctx->stream));
   TRY(cudaStreamSynchronize(ctx->stream));
@@ -831,7 +875,10 @@ int aco_b200_evaporate_deposit(aco_b200_ctx *ctx, int best_ant, float dep_iter,
     dn = ctx->d_tmp_nodes;
     dl = ctx->d_tmp_lens;
   }
-  TRY(launch_evap_deposit_explicit(ctx->iv, ctx->pv, ctx->ab, best_ant, dep_iter, dn, dl,
+  PheromoneView pv = ctx->pv;
+  int rc = current_tau(ctx, &pv.tau);
+  if (rc) return rc;
+  TRY(launch_evap_deposit_explicit(ctx->iv, pv, ctx->ab, best_ant, dep_iter, dn, dl,
                                    dep_global, ctx->d_counter, ctx->evap_grid, s));
   TRY(cudaStreamSynchronize(s));
   return ACO_OK;

@@ -404,7 +404,8 @@ def run_single(args, rank, world, local, torch, dist, _native):
             "wall_s": wall,
             "gpu_launches": 4 * args.steps,
             "kernels_us": {"weights": float(kms[0]) * 1e3, "construct": float(kms[1]) * 1e3,
-                           "best": float(kms[2]) * 1e3, "evap_deposit": float(kms[3]) * 1e3},
+                           "evaporate (beside construct in the graph)": float(kms[2]) * 1e3,
+                           "best_deposit": float(kms[3]) * 1e3},
             "kernel_share": {"construct": float(kms[1]) / total_k if total_k else None},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
@@ -511,7 +512,8 @@ def run_sharded(args, rank, world, local, torch, dist, _native):
         "wall_s": wall,
         "gpu_launches": 5 * args.steps,
         "kernels_us": {"weights": float(kms[0]) * 1e3, "construct": float(kms[1]) * 1e3,
-                       "best": float(kms[2]) * 1e3, "evap_deposit": float(kms[3]) * 1e3},
+                       "evaporate (beside construct in the graph)": float(kms[2]) * 1e3,
+                           "best_deposit": float(kms[3]) * 1e3},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
                      "traffic": CONSTRUCT_DRAM_BYTES_PER_LAUNCH.get(args.workload),

@@ -111,9 +111,10 @@ ACO_API int aco_b200_run(aco_b200_ctx *ctx, int max_epochs, aco_b200_state *stat
 ACO_API int aco_b200_enqueue_epochs(aco_b200_ctx *ctx, int epochs);
 ACO_API int aco_b200_synchronize(aco_b200_ctx *ctx);
 
-/* Runs `epochs` epochs with one CUDA event between consecutive kernels on
- * the context stream and adds each kernel's device time (ms) into
- * kernel_ms[4]: weights, construct, best, evaporate+deposit. */
+/* Runs `epochs` epochs, their kernels one after another with a CUDA event
+ * between consecutive kernels on the context stream (the epoch graph runs
+ * the evaporation beside the construction), and adds each kernel's device
+ * time (ms) into kernel_ms[4]: weights, construct, evaporate, best+deposit. */
 ACO_API int aco_b200_profile_epochs(aco_b200_ctx *ctx, int epochs, float *kernel_ms);
 
 /* Best solution so far in compact form: K segments [0 c.. 0] back to back

@@ -244,8 +244,8 @@ class Context:
         _check(self._lib.aco_b200_enqueue_epochs(self._h, epochs), "aco_b200_enqueue_epochs")
 
     def profile_epochs(self, epochs: int) -> np.ndarray:
-        """Per-kernel device ms summed over `epochs` epochs:
-        [weights, construct, best, evaporate+deposit]."""
+        """Per-kernel device ms summed over `epochs` epochs, the kernels run
+        one after another: [weights, construct, evaporate, best+deposit]."""
         ms = np.zeros(4, np.float32)
         _check(self._lib.aco_b200_profile_epochs(self._h, epochs, _p(ms)),
                "aco_b200_profile_epochs")

@@ -685,13 +685,11 @@ int aco_b200_profile_epochs(aco_b200_ctx *ctx, int epochs, float *kernel_ms) {
       err = launch_construct(ctx->iv, ctx->et, ctx->ab, ctx->plan, ctx->d_state, ctx->seed, 0, 0, 1, s);
     if (err == cudaSuccess) err = cudaEventRecord(ev[2], s);
     if (err == cudaSuccess)
-      err = launch_best(ctx->iv, ctx->ab, ctx->d_state, ctx->d_gbest_nodes, ctx->d_gbest_lens,
-                        ctx->d_log, s);
+      err = launch_evaporate_to(ctx->pv, ctx->d_tau2, ctx->d_state, ctx->evap_grid, s);
     if (err == cudaSuccess) err = cudaEventRecord(ev[3], s);
     if (err == cudaSuccess)
-      err = launch_evap_deposit(ctx->iv, ctx->pv, ctx->ab, ctx->d_state, ctx->d_gbest_nodes,
-                                ctx->d_gbest_lens, ctx->d_counter, ctx->evap_grid,
-                                ctx->d_tau2, s);
+      err = launch_best_deposit(ctx->iv, ctx->ab, ctx->pv, ctx->d_tau2, ctx->d_state,
+                                ctx->d_gbest_nodes, ctx->d_gbest_lens, ctx->d_log, s);
     if (err == cudaSuccess) err = cudaEventRecord(ev[4], s);
     if (err == cudaSuccess) err = cudaEventSynchronize(ev[4]);
     for (int i = 0; i < 4 && err == cudaSuccess; ++i) {

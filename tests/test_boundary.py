@@ -160,6 +160,20 @@ def test_parser_rejects_what_the_reference_rejects(native, tmp_path):
     assert _load(native, str(tmp_path / "missing.vrp"))[0] == 1
 
 
+def test_depot_section(native, tmp_path):
+    """DEPOT_SECTION naming node 1 is accepted; any other depot is refused by
+    both readers (every solver here, like the reference, has node 1 as depot)."""
+    base = SMOKE.split("EOF")[0].rstrip("\n") + "\n"
+    ok = base + "DEPOT_SECTION\n1\n-1\nEOF\n"
+    rc, (n, *_rest) = _load(native, _write(tmp_path, ok, "g.vrp"), demands=True)
+    assert rc == 0 and n == 8
+    assert I.read_vrp(_write(tmp_path, ok, "g2.vrp")).n == 8
+    other = base + "DEPOT_SECTION\n3\n-1\nEOF\n"
+    assert _load(native, _write(tmp_path, other, "h.vrp"), demands=True)[0] == 1
+    with pytest.raises(ValueError):
+        I.read_vrp(_write(tmp_path, other, "h2.vrp"))
+
+
 def test_cli_rejects_vehicle_mismatch(tmp_path):
     p = _write(tmp_path, SMOKE)
     r = subprocess.run([CLI, p, "3", "4"], capture_output=True, text=True)

@@ -3,6 +3,7 @@
  * as the reference (src/common/instance_parser.c:226-388): DIMENSION (n+1),
  * VEHICLES, CAPACITY ("KEY: v", "KEY : v" or "KEY v"), NODE_COORD_SECTION
  * ("id x y" for n+1 nodes, depot first) and DEMAND_SECTION ("id d").
+ * An optional DEPOT_SECTION ("1", "-1") may only name node 1.
  * Missing VEHICLES/CAPACITY/DEMAND_SECTION, a nonzero depot demand or a
  * non-positive capacity are errors, as in the reference.
  *
@@ -87,6 +88,17 @@ static int load(const char *path, int *n_out, float **xo, float **yo,
         }
       }
       have_demands = !err;
+    } else if (strncmp(line, "DEPOT_SECTION", 13) == 0) {
+      /* Depot ids up to -1: node 1 (index 0) must be the only depot, the
+       * layout every solver here and in the reference assumes. */
+      int id = 0, count = 0;
+      while (fscanf(f, "%d", &id) == 1 && id != -1) {
+        if (id != 1 || ++count > 1) {
+          fprintf(stderr, "Only node 1 may be the depot (DEPOT_SECTION) in %s\n", path);
+          err = 1;
+          break;
+        }
+      }
     }
   }
   fclose(f);

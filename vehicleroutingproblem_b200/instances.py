@@ -226,6 +226,13 @@ def read_vrp(path: str) -> Instance:
                 i += 1
                 parts = toks[i].split()
                 dem[j] = int(parts[1])
+        elif key == "DEPOT_SECTION":
+            depots = []
+            while i + 1 < len(toks) and toks[i + 1].strip() not in ("-1", "EOF"):
+                i += 1
+                depots.append(int(toks[i].split()[0]))
+            if depots and depots != [1]:
+                raise ValueError(f"{path}: only node 1 may be the depot (DEPOT_SECTION)")
         i += 1
     if xs is None or dem is None or n <= 0:
         raise ValueError(f"{path}: missing DIMENSION/NODE_COORD_SECTION/DEMAND_SECTION")

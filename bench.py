@@ -650,7 +650,8 @@ def run_batched(args, rank, world, local, torch, dist, _native):
 
 
 LEARNED = dict(train=4096, heldout=256, elite_ants=64, elite_k=16, elite_epochs=120,
-               train_epochs=10, batch=4096, lr=2e-3, gammas=(1.0, 2.0, 4.0), validation=8,
+               train_epochs=10, batch=4096, lr=2e-3, gammas=(2.0, 4.0, 6.0), validation=8,
+               control_betas=(3.0, 5.0, 8.0),
                epochs=300, ants=256, cand_k=32,
                name="learned prior: 4096 training instances n~U[200,1000] (seed 40000), "
                     "256 held-out n=1000 K=8 (seeds 50000-50255), 256 ants 32-NN, "
@@ -684,17 +685,23 @@ def run_learned(args, rank, world, local, torch, dist, _native):
     t0 = time.perf_counter()
     losses = pr.train(L["train_epochs"], batch=L["batch"], lr=L["lr"], seed=11)
     train_s = time.perf_counter() - t0
+    # gamma for the learned levels, and the control's beta (the plain solver
+    # with a sharper hand-set eta^beta), each chosen on 8 validation
+    # instances by the mean final cost relative to the plain solver.
     val = [I.uniform_instance(1000, 8, 60000 + i) for i in range(L["validation"])]
-    scores = {}
-    for g in L["gammas"]:
-        r = PR.time_to_cost(val, pr, gamma=g, epochs=L["epochs"], ants=L["ants"],
-                            cand_k=L["cand_k"])
-        scores[g] = r["time_ratio_of_sums"]
+    base = PR.final_costs(val, L["epochs"], ants=L["ants"], cand_k=L["cand_k"])
+    scores = {g: float(np.mean(PR.final_costs(val, L["epochs"], pr, g, ants=L["ants"],
+                                              cand_k=L["cand_k"]) / base))
+              for g in L["gammas"]}
     gamma = min(scores, key=lambda g: scores[g])
+    ctrl = {b: float(np.mean(PR.final_costs(val, L["epochs"], beta=b, ants=L["ants"],
+                                            cand_k=L["cand_k"]) / base))
+            for b in L["control_betas"]}
+    beta_c = min(ctrl, key=lambda b: ctrl[b])
     held = I.prior_heldout_instances(nheld)
     t0 = time.perf_counter()
     res = PR.time_to_cost(held, pr, gamma=gamma, epochs=L["epochs"], ants=L["ants"],
-                          cand_k=L["cand_k"])
+                          cand_k=L["cand_k"], control_beta=beta_c)
     eval_s = time.perf_counter() - t0
     rows = res.pop("rows")
     flops = TRAIN_FLOPS_PER_EDGE * 32.0 * count * L["train_epochs"]
@@ -713,7 +720,8 @@ def run_learned(args, rank, world, local, torch, dist, _native):
         "dtype": "bf16 MLP (fp32 accumulate) + int32 weights + u8 pheromone",
         "data": "synthetic",
         "config": {"workload": L["name"], "train_instances": ntrain, "heldout": nheld,
-                   "gamma": gamma, "gamma_validation": scores},
+                   "gamma": gamma, "gamma_validation_final_cost": scores,
+                   "control_beta": beta_c, "control_validation_final_cost": ctrl},
         "time_to_cost": res,
         "training": {"examples": count, "epochs": L["train_epochs"], "batch": L["batch"],
                      "lr": L["lr"], "loss_first_last": [float(losses[0]), float(losses[-1])],

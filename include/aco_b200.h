@@ -229,6 +229,11 @@ ACO_API int aco_b200_prior_get_examples(aco_b200_prior *prior, int *rows_slots, 
 ACO_API int aco_b200_prior_get_rows(aco_b200_prior *prior, long long first, int count,
                                     uint16_t *features, uint8_t *kv, float *scores);
 ACO_API int aco_b200_apply_prior(aco_b200_ctx *ctx, aco_b200_prior *prior, float gamma);
+/* mode 0: as aco_b200_apply_prior (learned levels replace the plain ones);
+ * mode 1: residual, learned levels added to the plain eta^beta levels
+ * (weights proportional to tau^alpha eta^beta exp(gamma s)). */
+ACO_API int aco_b200_apply_prior_mode(aco_b200_ctx *ctx, aco_b200_prior *prior, float gamma,
+                                      int mode);
 
 /*
  * Batched solving: many independent instances in one persistent launch.

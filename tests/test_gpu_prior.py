@@ -235,3 +235,22 @@ def test_time_to_cost_pipeline(dataset):
     row = res["rows"][0]
     assert res["instances"] == 1 and 1 <= row["plain_epochs"] <= 30
     assert row["plain_s"] > 0 and row["learned_s"] > 0 and row["prior_s"] > 0
+
+
+def test_residual_levels_add_to_plain(dataset, native):
+    from oracle import prior_oracle as PO
+    insts, _, pr, _, offs = dataset
+    inst, off = insts[1], int(offs[1])
+    _, kv, sc = pr.rows(off, inst.n + 1, scores=True)
+    with native.Context(0) as c:
+        c.setup_instance(inst, ants=16, cand_k=K_CAND, seed=3)
+        _, plain = c.candidates()
+        c.apply_prior(pr, 2.0, residual=True)
+        _, lvl = c.candidates()
+        learned = PO.levels(sc, kv, K_CAND, 2.0)
+        plain = plain.reshape(-1, K_CAND).astype(np.int64)
+        valid = np.arange(K_CAND)[None, :] < kv[:, None]
+        exp = np.where(valid, np.minimum(4095, plain + learned), 4095)
+        assert np.array_equal(lvl.reshape(-1, K_CAND).astype(np.int64), exp)
+        c.apply_prior(pr, 2.0, residual=True)  # applying again starts from the plain levels
+        assert np.array_equal(c.candidates()[1], lvl)

@@ -45,7 +45,7 @@ EXPORTED = [
     "aco_b200_prior_load", "aco_b200_prior_save", "aco_b200_prior_set_dataset",
     "aco_b200_prior_train", "aco_b200_prior_gradient", "aco_b200_prior_num_examples",
     "aco_b200_prior_get_examples", "aco_b200_prior_get_rows", "aco_b200_apply_prior",
-    "aco_b200_batch_apply_prior",
+    "aco_b200_batch_apply_prior", "aco_b200_apply_prior_mode",
     "aco_status_string", "aco_vrp_cuda_with_capacity", "aco_vrp_cuda_with_demands",
     "solution_create", "solution_free", "solution_reset", "solution_copy",
     "solution_cost", "route_append", "solution_validate",
@@ -148,6 +148,7 @@ def load():
         "aco_b200_prior_get_examples": [vp, vp, C.c_longlong],
         "aco_b200_prior_get_rows": [vp, C.c_longlong, i32, vp, vp, vp],
         "aco_b200_apply_prior": [vp, vp, f32],
+        "aco_b200_apply_prior_mode": [vp, vp, f32, i32],
         "aco_b200_batch_apply_prior": [vp, vp, f32],
     }
     for name, args in sigs.items():
@@ -354,10 +355,13 @@ class Context:
         _check(self._lib.aco_b200_shard_update(self._h, C.c_void_p(d_recv), world),
                "aco_b200_shard_update")
 
-    def apply_prior(self, prior: Optional["Prior"], gamma: float = 1.0) -> None:
-        """Learned eta levels from `prior` (None or gamma <= 0: plain levels)."""
-        _check(self._lib.aco_b200_apply_prior(self._h, prior._h if prior else None, gamma),
-               "aco_b200_apply_prior")
+    def apply_prior(self, prior: Optional["Prior"], gamma: float = 1.0,
+                    residual: bool = False) -> None:
+        """Learned eta levels from `prior` (None or gamma <= 0: plain levels);
+        residual: added to the plain levels instead of replacing them."""
+        _check(self._lib.aco_b200_apply_prior_mode(self._h, prior._h if prior else None, gamma,
+                                                   1 if residual else 0),
+               "aco_b200_apply_prior_mode")
 
 
 PRIOR_PARAMS = 4801

@@ -1009,7 +1009,7 @@ extern "C" int aco_b200_batch_apply_prior(aco_b200_batch *b, aco_b200_prior *pri
     if (prior && gamma > 0.f) {
       int rc = acob200::prior::learned_levels(prior, a.coords + I.node_off, a.demand + I.node_off,
                                               I.cap, I.n, b->k, a.cand + I.node_off * b->k,
-                                              lvl + I.node_off * b->k, gamma, s);
+                                              lvl + I.node_off * b->k, gamma, 0, s);
       if (rc) return rc;
     } else {
       BTRY(launch_knn_levels(a.coords + I.node_off, I.n, b->k, b->d_thr, kThresholds,

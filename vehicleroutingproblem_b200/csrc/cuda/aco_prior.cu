@@ -544,8 +544,10 @@ __global__ void k_prior_adam(float *params, float *m, float *v, float *grad, int
 }
 
 // Levels from scores: warp per row, L = min(4095, round(scale (s_max - s))).
+// residual: the learned level is added to the plain level already in lvl
+// (weights proportional to eta^beta exp(gamma s)).
 __global__ void k_prior_levels(const float *scores, const uint8_t *kv, int rows, int k,
-                               float scale, uint16_t *lvl) {
+                               float scale, int residual, uint16_t *lvl) {
   const int lane = threadIdx.x & 31;
   const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (row >= rows) return;
@@ -554,7 +556,10 @@ __global__ void k_prior_levels(const float *scores, const uint8_t *kv, int rows,
   const float mx = warp_max(valid ? s : -FLT_MAX);
   if (lane < k) {
     int L = kThresholds;
-    if (valid) L = (int)fminf((float)kThresholds, rintf(scale * (mx - s)));
+    if (valid) {
+      L = (int)fminf((float)kThresholds, rintf(scale * (mx - s)));
+      if (residual) L = min(kThresholds, L + (int)lvl[(size_t)row * k + lane]);
+    }
     lvl[(size_t)row * k + lane] = (uint16_t)L;
   }
 }
@@ -692,7 +697,7 @@ static int launch_features(aco_b200_prior *p, const float2 *coords, const int *d
 
 int learned_levels(aco_b200_prior *p, const float2 *coords, const int *demand, long long cap,
                    int n, int k, const uint16_t *cand, uint16_t *lvl, float gamma,
-                   cudaStream_t s) {
+                   int residual, cudaStream_t s) {
   if (!p || k < 1 || k > kSlots || n < 1) return ACO_ERR_INVALID_INPUT;
   const long long rows = (long long)n + 1;
   int rc = ensure_scratch(p, rows);
@@ -703,7 +708,7 @@ int learned_levels(aco_b200_prior *p, const float2 *coords, const int *demand, l
   if (rc) return rc;
   const float scale = gamma * (float)kLevelsPerOctave / logf(2.0f);
   k_prior_levels<<<(unsigned)((rows + 7) / 8), 256, 0, s>>>(p->d_sscores, p->d_skv, (int)rows, k,
-                                                           scale, lvl);
+                                                           scale, residual, lvl);
   PTRY(cudaGetLastError());
   return ACO_OK;
 }

@@ -621,20 +621,26 @@ int aco_b200_get_depot_tables(aco_b200_ctx *ctx, uint16_t *lvl0, int32_t *rdep, 
   return ACO_OK;
 }
 
-int aco_b200_apply_prior(aco_b200_ctx *ctx, aco_b200_prior *prior, float gamma) {
-  if (!ctx || !ctx->ready) return ACO_ERR_INVALID_INPUT;
+int aco_b200_apply_prior_mode(aco_b200_ctx *ctx, aco_b200_prior *prior, float gamma,
+                              int mode) {
+  if (!ctx || !ctx->ready || mode < 0 || mode > 1) return ACO_ERR_INVALID_INPUT;
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
+  // Plain levels first: they are the result without a prior and the base of
+  // the residual mode.
+  TRY(launch_knn_levels(ctx->d_coords, ctx->n, ctx->k, ctx->d_thr, kThresholds, ctx->d_cand,
+                        ctx->d_lvl, s));
   if (prior && gamma > 0.f) {
     int rc = acob200::prior::learned_levels(prior, ctx->d_coords, ctx->d_demand, ctx->cap, ctx->n,
-                                            ctx->k, ctx->d_cand, ctx->d_lvl, gamma, s);
+                                            ctx->k, ctx->d_cand, ctx->d_lvl, gamma, mode, s);
     if (rc) return rc;
-  } else {
-    TRY(launch_knn_levels(ctx->d_coords, ctx->n, ctx->k, ctx->d_thr, kThresholds, ctx->d_cand,
-                          ctx->d_lvl, s));
   }
   TRY(cudaStreamSynchronize(s));
   return ACO_OK;
+}
+
+int aco_b200_apply_prior(aco_b200_ctx *ctx, aco_b200_prior *prior, float gamma) {
+  return aco_b200_apply_prior_mode(ctx, prior, gamma, 0);
 }
 
 int aco_b200_shard_packet_ints(aco_b200_ctx *ctx) {

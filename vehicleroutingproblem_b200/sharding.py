@@ -123,15 +123,24 @@ class ShardedColony:
         self.world = dist.get_world_size(group)
         self.device = torch.device("cuda", device)
         self.stream = stream if stream is not None else torch.cuda.Stream(self.device)
-        params = dict(params)
-        self.timeout_seconds = float(params.pop("timeout_seconds", 0.0) or 0.0)
+        self.ants = ants
         self.ctx = N.Context(device)
         self.ctx.set_stream(self.stream.cuda_stream)
-        self.ctx.setup_instance(inst, ants=ants, ant_base=self.rank * ants,
+        self.send = self.recv = None
+        self.setup(inst, **params)
+
+    def setup(self, inst, **params) -> None:
+        """(Re)starts the colony on an instance; the context's device buffers
+        and the packet buffers are reused when the sizes are unchanged."""
+        import torch
+        params = dict(params)
+        self.timeout_seconds = float(params.pop("timeout_seconds", 0.0) or 0.0)
+        self.ctx.setup_instance(inst, ants=self.ants, ant_base=self.rank * self.ants,
                                 timeout_seconds=0.0, **params)
         P = self.ctx.shard_packet_ints()
-        self.send = torch.zeros(P, dtype=torch.int32, device=self.device)
-        self.recv = torch.zeros(self.world * P, dtype=torch.int32, device=self.device)
+        if self.send is None or self.send.numel() != P:
+            self.send = torch.zeros(P, dtype=torch.int32, device=self.device)
+            self.recv = torch.zeros(self.world * P, dtype=torch.int32, device=self.device)
         self._t0 = time.monotonic()
 
     def close(self) -> None:

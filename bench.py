@@ -80,6 +80,7 @@ BATCHED = dict(count=512, seed0=30000, ants=64, cand_k=16, epochs=300,
 CONSTRUCT_DRAM_BYTES_PER_LAUNCH = {"n1000": 234496}
 OMP_BIN = os.path.join(ROOT, "oracle", "_ref", "aco_vrp_omp.out")
 REF_CUDA_BIN = os.path.join(ROOT, "oracle", "_ref", "aco_vrp_cuda_ref.out")
+SEQ_BIN = os.path.join(ROOT, "oracle", "_ref", "aco_vrp_seq.out")
 OUR_CLI = os.path.join(ROOT, "aco_vrp_cuda.out")
 CLI_SECONDS = 4.0
 
@@ -303,6 +304,12 @@ def run_reference_arm(args, rank, world):
                     "d2h_bytes_per_step": 0}}
     if ref_gpu is not None:
         line["reference_cuda_same_gpu"] = ref_gpu
+    if args.workload != "batched" and os.path.exists(SEQ_BIN):
+        # The reference's sequential solver on one host core, same CLI.
+        try:
+            line["reference_seq_1core"] = cli_epoch_rate(SEQ_BIN, inst, wl["ants"], seconds=10.0)
+        except Exception as exc:  # reported, not fatal
+            line["reference_seq_1core"] = {"error": str(exc)[:200]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -397,6 +404,7 @@ def run_single(args, rank, world, local, torch, dist, _native):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "int32 weights + u8 pheromone (f64 route costs)",
             "data": "synthetic",
+            "solutions_per_s": world * m * args.steps / (dev_ms_max / 1e3),
             "config": {"workload": wl["name"], "n": n, "K": K, "capacity": inst.capacity,
                        "ants": m, "cand_k": k, "step": "one epoch",
                        "l2": "flushed between timed steps (256 MiB write outside the events)",

@@ -12,7 +12,7 @@ The pipeline the prior is built with:
    (`Prior.train`);
 4. use -- `Context.apply_prior(prior, gamma)` replaces the eta levels of an
    instance by the learned ones; the plain levels stay the fallback;
-5. judgement -- `time_to_cost`: on held-out instances, the time the learned
+5. evaluation -- `time_to_cost`: on held-out instances, the time the learned
    prior needs to reach the plain solver's final cost (+0.5%), FP64 costs,
    against the time the plain solver needs.
 """

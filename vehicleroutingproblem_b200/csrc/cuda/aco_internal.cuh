@@ -190,13 +190,7 @@ cudaError_t launch_shard_pack(const InstanceView &iv, const AntBuffers &ab, DevS
 cudaError_t launch_shard_select(const InstanceView &iv, DevState *st, const int *recv,
                                 int world, int *iter_nodes, int *iter_lens,
                                 int *gbest_nodes, int *gbest_lens, EpochRec *log,
-                                cudaStream_t s);
-cudaError_t launch_evap_deposit_iter(const InstanceView &iv, const PheromoneView &pv,
-                                     const AntBuffers &ab, DevState *st,
-                                     const int *iter_nodes, const int *iter_lens,
-                                     const int *gbest_nodes, const int *gbest_lens,
-                                     unsigned int *counter, int grid, uint8_t *tau_alt,
-                                     cudaStream_t s);
+                                const PheromoneView &pv, uint8_t *tau_alt, cudaStream_t s);
 int construct_max_smem();
 cudaError_t prepare_construct_kernels();
 SmemPlan plan_construct(const InstanceView &iv, int layout, int num_sms,

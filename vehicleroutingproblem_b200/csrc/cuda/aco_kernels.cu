@@ -1004,8 +1004,6 @@ struct EvapArgs {
   DevState *st;
   const int *gbest_nodes;
   const int *gbest_lens;
-  const int *iter_nodes;  // iteration best from an exchange (else best ant's)
-  const int *iter_lens;
   unsigned int *counter;
   int best_ant;          // used when st == nullptr
   float dep_iter, dep_global;
@@ -1063,11 +1061,8 @@ __global__ void __launch_bounds__(512) k_evap_deposit(EvapArgs a) {
   const float dep_g = a.st ? a.st->dep_global : a.dep_global;
   extern __shared__ int s_off[];
   int *offs = (a.iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
-  if (a.iter_nodes)
-    deposit_solution(pv, stride_n, CompactNodes{a.iter_nodes}, a.iter_lens, a.iv.K, dep_i, offs);
-  else
-    deposit_solution(pv, stride_n, CompactNodes{a.ab.routes + (size_t)best * a.iv.route_stride},
-                     a.ab.lens + (size_t)best * a.iv.K, a.iv.K, dep_i, offs);
+  deposit_solution(pv, stride_n, CompactNodes{a.ab.routes + (size_t)best * a.iv.route_stride},
+                   a.ab.lens + (size_t)best * a.iv.K, a.iv.K, dep_i, offs);
   __syncthreads();
   if (a.gbest_nodes) {
     deposit_solution(pv, stride_n, CompactNodes{a.gbest_nodes}, a.gbest_lens, a.iv.K, dep_g, offs);
@@ -1087,8 +1082,6 @@ cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
   a.st = st;
   a.gbest_nodes = gbest_nodes;
   a.gbest_lens = gbest_lens;
-  a.iter_nodes = nullptr;
-  a.iter_lens = nullptr;
   a.counter = counter;
   a.best_ant = 0;
   a.dep_iter = a.dep_global = 0.0f;
@@ -1115,8 +1108,6 @@ cudaError_t launch_evap_deposit_explicit(const InstanceView &iv,
   a.st = nullptr;
   a.gbest_nodes = gbest_nodes;
   a.gbest_lens = gbest_lens;
-  a.iter_nodes = nullptr;
-  a.iter_lens = nullptr;
   a.counter = counter;
   a.best_ant = best_ant;
   a.dep_iter = dep_iter;
@@ -1212,12 +1203,14 @@ __global__ void __launch_bounds__(1024) k_shard_pack(InstanceView iv, AntBuffers
 // Winner over the gathered packets (lowest cost, then lowest global ant:
 // the first minimum a single device holding every ant would find), then the
 // same bookkeeping as k_best; its route goes to iter_nodes/iter_lens and,
-// on improvement, to the global best.
+// on improvement, to the global best; then both deposits into the
+// evaporated pheromone buffer and the buffer switch.
 __global__ void __launch_bounds__(256) k_shard_select(InstanceView iv, DevState *st,
                                                       const int *recv, int world,
                                                       int *iter_nodes, int *iter_lens,
                                                       int *gbest_nodes, int *gbest_lens,
-                                                      EpochRec *log) {
+                                                      EpochRec *log,
+                                                      PheromoneView pv, uint8_t *tau_alt) {
   if (*(volatile int *)&st->skip) return;
   __shared__ int s_src, s_improved;
   const int P = shard_packet_ints(iv.n, iv.K);
@@ -1254,6 +1247,22 @@ __global__ void __launch_bounds__(256) k_shard_select(InstanceView iv, DevState 
     iter_nodes[t] = pk[6 + iv.K + t];
     if (s_improved) gbest_nodes[t] = pk[6 + iv.K + t];
   }
+  // Deposits into the buffer the side stream evaporated into during the
+  // construction, then the switch (as k_best_t<true>).
+  __syncthreads();
+  const bool sel = *(volatile int *)&st->tau_sel != 0;
+  PheromoneView pd = pv;
+  pd.tau = sel ? pv.tau : tau_alt;
+  const size_t stride_n = (size_t)iv.n + 1;
+  extern __shared__ int s_off[];
+  int *offs = (iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
+  const float dep_i = *(volatile float *)&st->dep_iter;
+  const float dep_g = *(volatile float *)&st->dep_global;
+  deposit_solution(pd, stride_n, CompactNodes{iter_nodes}, iter_lens, iv.K, dep_i, offs);
+  __syncthreads();
+  deposit_solution(pd, stride_n, CompactNodes{gbest_nodes}, gbest_lens, iv.K, dep_g, offs);
+  __syncthreads();
+  if (threadIdx.x == 0) st->tau_sel = sel ? 0 : 1;
 }
 
 int shard_packet_size(int n, int K) { return shard_packet_ints(n, K); }
@@ -1267,33 +1276,10 @@ cudaError_t launch_shard_pack(const InstanceView &iv, const AntBuffers &ab, DevS
 cudaError_t launch_shard_select(const InstanceView &iv, DevState *st, const int *recv,
                                 int world, int *iter_nodes, int *iter_lens,
                                 int *gbest_nodes, int *gbest_lens, EpochRec *log,
-                                cudaStream_t s) {
-  k_shard_select<<<1, 256, 0, s>>>(iv, st, recv, world, iter_nodes, iter_lens, gbest_nodes,
-                                   gbest_lens, log);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_evap_deposit_iter(const InstanceView &iv, const PheromoneView &pv,
-                                     const AntBuffers &ab, DevState *st,
-                                     const int *iter_nodes, const int *iter_lens,
-                                     const int *gbest_nodes, const int *gbest_lens,
-                                     unsigned int *counter, int grid, uint8_t *tau_alt,
-                                     cudaStream_t s) {
-  EvapArgs a;
-  a.iv = iv;
-  a.pv = pv;
-  a.ab = ab;
-  a.st = st;
-  a.gbest_nodes = gbest_nodes;
-  a.gbest_lens = gbest_lens;
-  a.iter_nodes = iter_nodes;
-  a.iter_lens = iter_lens;
-  a.counter = counter;
-  a.best_ant = 0;
-  a.dep_iter = a.dep_global = 0.0f;
-  a.tau_alt = tau_alt;
+                                const PheromoneView &pv, uint8_t *tau_alt, cudaStream_t s) {
   const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
-  k_evap_deposit<<<grid, 512, smem, s>>>(a);
+  k_shard_select<<<1, 256, smem, s>>>(iv, st, recv, world, iter_nodes, iter_lens, gbest_nodes,
+                                      gbest_lens, log, pv, tau_alt);
   return cudaGetLastError();
 }
 

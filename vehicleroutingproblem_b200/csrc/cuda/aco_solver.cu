@@ -656,9 +656,16 @@ int aco_b200_shard_construct(aco_b200_ctx *ctx, int32_t *d_send) {
     TRY(launch_set_run_limit(ctx->d_state, 0, s));
     ctx->run_limit_off = true;
   }
+  // As in the epoch graph: the evaporation into the other pheromone buffer
+  // runs on the side stream beside the construction.
   TRY(launch_weights(ctx->iv, ctx->pv, ctx->et, ctx->d_state, s));
+  TRY(cudaEventRecord(ctx->ev_fork, s));
+  TRY(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+  TRY(launch_evaporate_to(ctx->pv, ctx->d_tau2, ctx->d_state, ctx->evap_grid, ctx->side));
   TRY(launch_construct(ctx->iv, ctx->et, ctx->ab, ctx->plan, ctx->d_state, ctx->seed, 0, 0, 1, s));
   TRY(launch_shard_pack(ctx->iv, ctx->ab, ctx->d_state, d_send, s));
+  TRY(cudaEventRecord(ctx->ev_join, ctx->side));
+  TRY(cudaStreamWaitEvent(s, ctx->ev_join, 0));
   return ACO_OK;
 }
 
@@ -667,10 +674,8 @@ int aco_b200_shard_update(aco_b200_ctx *ctx, const int32_t *d_recv, int world) {
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
   TRY(launch_shard_select(ctx->iv, ctx->d_state, d_recv, world, ctx->d_iter_nodes,
-                          ctx->d_iter_lens, ctx->d_gbest_nodes, ctx->d_gbest_lens, ctx->d_log, s));
-  TRY(launch_evap_deposit_iter(ctx->iv, ctx->pv, ctx->ab, ctx->d_state, ctx->d_iter_nodes,
-                               ctx->d_iter_lens, ctx->d_gbest_nodes, ctx->d_gbest_lens,
-                               ctx->d_counter, ctx->evap_grid, ctx->d_tau2, s));
+                          ctx->d_iter_lens, ctx->d_gbest_nodes, ctx->d_gbest_lens, ctx->d_log,
+                          ctx->pv, ctx->d_tau2, s));
   return ACO_OK;
 }
 

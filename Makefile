@@ -25,7 +25,7 @@ C_SRCS := $(CSRC)/common/solution.c $(CSRC)/common/instance_parser.c \
           $(CSRC)/common/aco_config.c $(CSRC)/common/cli_common.c
 CU_OBJS := $(patsubst $(CSRC)/cuda/%.cu,$(BUILD)/%.o,$(CU_SRCS))
 C_OBJS := $(patsubst $(CSRC)/common/%.c,$(BUILD)/%.o,$(C_SRCS))
-HDRS := $(wildcard include/*.h) $(CSRC)/cuda/aco_internal.cuh
+HDRS := $(wildcard include/*.h) $(wildcard $(CSRC)/cuda/*.cuh) $(wildcard $(CSRC)/cuda/*.h)
 
 all: lib cuda
 

@@ -132,6 +132,15 @@ ACO_API int aco_b200_get_tables(aco_b200_ctx *ctx, int32_t *A, uint32_t *lut,
                         float *thresholds, int n_thresholds);
 /* Weights recomputed from the current pheromone ((n+1) k values). */
 ACO_API int aco_b200_get_weights(aco_b200_ctx *ctx, uint32_t *w);
+/* Fault-injection test hooks (host-made failures; no GPU fault):
+ *   what 1: the value-th device allocation of the following set-up fails as
+ *           out of memory (0 = off) -- set-up must return ACO_ERR_ALLOCATION
+ *           and free what it allocated;
+ *   what 2: value 1 makes the construct kernel's bounded wait for its staged
+ *           tables run out (the wait expects 16 bytes more than it copies):
+ *           the kernel flags the error and returns, and aco_b200_run returns
+ *           ACO_ERR_BACKEND; value 0 restores it (a set-up clears the flag). */
+ACO_API int aco_b200_debug_inject(aco_b200_ctx *ctx, int what, int value);
 /* Depot rule 1 only: eta level of d(i,0)^2 per node, the last weights
  * pass's depot-close levels rdep[n+1] and the depot factor's level e_dep. */
 ACO_API int aco_b200_get_depot_tables(aco_b200_ctx *ctx, uint16_t *lvl0, int32_t *rdep,

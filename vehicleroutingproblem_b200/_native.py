@@ -39,7 +39,7 @@ EXPORTED = [
     "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
     "aco_b200_batch_get", "aco_b200_batch_get_costs",
     "aco_b200_shard_packet_ints", "aco_b200_shard_construct", "aco_b200_shard_update",
-    "aco_b200_get_depot_tables",
+    "aco_b200_get_depot_tables", "aco_b200_debug_inject",
     "aco_b200_prior_create", "aco_b200_prior_destroy", "aco_b200_prior_set_stream",
     "aco_b200_prior_init", "aco_b200_prior_set_params", "aco_b200_prior_get_params",
     "aco_b200_prior_load", "aco_b200_prior_save", "aco_b200_prior_set_dataset",
@@ -138,6 +138,7 @@ def load():
         "aco_b200_shard_packet_ints": [vp], "aco_b200_shard_construct": [vp, vp],
         "aco_b200_shard_update": [vp, vp, i32],
         "aco_b200_get_depot_tables": [vp, vp, vp, vp],
+        "aco_b200_debug_inject": [vp, i32, i32],
         "aco_b200_prior_create": [vp, i32], "aco_b200_prior_destroy": [vp],
         "aco_b200_prior_set_stream": [vp, vp], "aco_b200_prior_init": [vp, C.c_uint],
         "aco_b200_prior_set_params": [vp, vp, i32], "aco_b200_prior_get_params": [vp, vp, i32],
@@ -300,6 +301,12 @@ class Context:
         w = np.zeros((self.n + 1) * self.k, np.uint32)
         _check(self._lib.aco_b200_get_weights(self._h, _p(w)), "aco_b200_get_weights")
         return w
+
+    def debug_inject(self, what: int, value: int) -> None:
+        """Fault-injection test hook (aco_b200_debug_inject): what 1 fails the
+        value-th device allocation of the next set-up; what 2 makes the
+        construct kernel's staging wait run out (value 1) or not (0)."""
+        _check(self._lib.aco_b200_debug_inject(self._h, what, value), "aco_b200_debug_inject")
 
     def depot_tables(self):
         """Reference-CUDA depot rule: (lvl0 [n+1], rdep [n+1] of the last

@@ -114,6 +114,7 @@ struct InstanceView {
   int route_stride;        // n + 2K
   int ant_base;            // global id of local ant 0 (colony split over devices)
   int depot_rule;          // kDepotRuleSeq or kDepotRuleCudaRef
+  int stage_extra_tx;      // test hook: bytes the staging wait expects beyond the copies
   const float2 *coords;    // [n+1]
   const int *demand;       // [n+1]
   const uint16_t *cand;    // [(n+1) k]

@@ -576,7 +576,7 @@ __global__ void __launch_bounds__(512, 1) k_construct(ConstructArgs a) {
     __syncthreads();
     if (threadIdx.x == 0) {
       const uint32_t total = pl.bytes_cand + pl.bytes_w + pl.bytes_coords + (UNIT ? 0u : pl.bytes_dem);
-      mbar_arrive_expect_tx(bar, total);
+      mbar_arrive_expect_tx(bar, total + (uint32_t)iv.stage_extra_tx);
       const uint32_t kChunk = 32768u;
       auto issue = [&](unsigned char *dst, const void *src, uint32_t bytes) {
         const unsigned char *sp = reinterpret_cast<const unsigned char *>(src);
@@ -604,8 +604,12 @@ __global__ void __launch_bounds__(512, 1) k_construct(ConstructArgs a) {
            pl.vis_words, iv.n, lane);
 
   if (L != kLayoutGlobal) {
-    if (!mbar_wait_bounded(bar, 0, 1u << 22)) {
+    // Bounded wait for the staged tables; on time-out the block flags the
+    // error, waits (bounded again) for its copies still in flight and exits.
+    const uint32_t limit = iv.stage_extra_tx ? (1u << 14) : (1u << 22);
+    if (!mbar_wait_bounded(bar, 0, limit)) {
       if (lane == 0 && a.st) atomicOr(&a.st->error, kErrStageTimeout);
+      mbar_wait_bounded(bar, 0, limit);
       return;
     }
   }

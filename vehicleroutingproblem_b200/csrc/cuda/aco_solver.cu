@@ -107,6 +107,7 @@ struct aco_b200_ctx {
   cudaGraphExec_t graph_one = nullptr;
   bool run_limit_off = false;  // device run limit known to be disabled
   int depot_rule = 0;
+  int inject_alloc = 0;  // test hook: the n-th device allocation of a set-up fails
   // Kernel arguments the graphs were captured with: a set-up that leaves
   // them unchanged (same sizes, parameters and buffers) keeps the graphs.
   unsigned char graph_key[sizeof(InstanceView) + sizeof(PheromoneView) + sizeof(EpochTables) +
@@ -179,7 +180,9 @@ aco_b200_ctx::~aco_b200_ctx() {
 
 #define TRY_ALLOC(call)                                                  \
   do {                                                                   \
-    cudaError_t err__ = (call);                                          \
+    cudaError_t err__ = (ctx->inject_alloc > 0 && --ctx->inject_alloc == 0) \
+                            ? cudaErrorMemoryAllocation                  \
+                            : (call);                                    \
     if (err__ != cudaSuccess) {                                          \
       fprintf(stderr, "aco_b200: device allocation failed: %s\n",       \
               cudaGetErrorString(err__));                                \
@@ -451,6 +454,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   iv.max_demand = max_demand;
   iv.route_stride = R;
   iv.ant_base = p->ant_base;
+  iv.stage_extra_tx = 0;
   iv.depot_rule = p->depot_rule;
   iv.coords = ctx->d_coords;
   iv.demand = ctx->d_demand;
@@ -608,6 +612,24 @@ int aco_b200_enqueue_epochs(aco_b200_ctx *ctx, int epochs) {
   }
   for (int i = 0; i < left; ++i) TRY(cudaGraphLaunch(ctx->graph_one, s));
   return ACO_OK;
+}
+
+int aco_b200_debug_inject(aco_b200_ctx *ctx, int what, int value) {
+  if (!ctx || value < 0) return ACO_ERR_INVALID_INPUT;
+  if (what == 1) {
+    ctx->inject_alloc = value;
+    return ACO_OK;
+  }
+  if (what == 2) {
+    cudaSetDevice(ctx->device);
+    ctx->iv.stage_extra_tx = value ? 16 : 0;
+    if (ctx->graph_chunk) cudaGraphExecDestroy(ctx->graph_chunk);
+    if (ctx->graph_one) cudaGraphExecDestroy(ctx->graph_one);
+    ctx->graph_chunk = ctx->graph_one = nullptr;
+    memset(ctx->graph_key, 0, sizeof(ctx->graph_key));
+    return ACO_OK;
+  }
+  return ACO_ERR_INVALID_INPUT;
 }
 
 int aco_b200_get_depot_tables(aco_b200_ctx *ctx, uint16_t *lvl0, int32_t *rdep, int *e_dep) {

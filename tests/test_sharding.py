@@ -165,3 +165,40 @@ def test_two_gloo_ranks_equal_one_colony(oracle_mod, tmp_path):
             col.update(r[3], r[1], r[2])
         assert np.array_equal(r0["taus"][e], col.tau)
     assert found_any
+
+
+def _leaving_worker(rank, world, port, out_dir):
+    import time
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=timedelta(seconds=5))
+    n, K = 10, 2
+    P = S.packet_ints(n, K)
+    send = torch.from_numpy(S.encode_packet(n, K, False, 0.0, 0, rank))
+    recv = torch.zeros(world * P, dtype=torch.int32)
+    S.exchange(send, recv)  # epoch 1: both ranks
+    if rank == 1:
+        os._exit(0)  # leaves between epochs, with no collective in flight
+    t0 = time.monotonic()
+    try:
+        S.exchange(send, recv)  # epoch 2: the peer is gone
+        outcome = "no error"
+    except Exception as exc:  # the process group reports the lost rank
+        outcome = "error: " + type(exc).__name__
+    with open(os.path.join(out_dir, "rank0.txt"), "w") as f:
+        f.write(f"{outcome}\n{time.monotonic() - t0:.3f}\n")
+    os._exit(0)
+
+
+@pytest.mark.timeout(120)
+def test_lost_rank_is_reported_not_waited_for(tmp_path):
+    """A rank that leaves between epochs: the other rank's next packet
+    exchange ends with an error within the process group's timeout."""
+    import torch.multiprocessing as mp
+    mp.spawn(_leaving_worker, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    outcome, secs = (tmp_path / "rank0.txt").read_text().splitlines()[:2]
+    assert outcome.startswith("error"), outcome
+    assert float(secs) < 30.0

@@ -149,6 +149,12 @@ ACO_API int aco_b200_get_depot_tables(aco_b200_ctx *ctx, uint16_t *lvl0, int32_t
  * per-ant results through aco_b200_get_ants.  layout: -1 = automatic,
  * 0 = shared-memory weights, 1 = shared-memory packed levels, 2 = global. */
 ACO_API int aco_b200_construct(aco_b200_ctx *ctx, int epoch, int layout);
+/* One construct pass that takes its random draws from a recorded stream
+ * (draws[ant * per_ant + d], the low 24 bits used; draws past per_ant read as
+ * 0) instead of Philox -- for parity against the reference's own
+ * construction fed the same stream.  Results through aco_b200_get_ants. */
+ACO_API int aco_b200_construct_with_draws(aco_b200_ctx *ctx, const uint32_t *draws,
+                                          int per_ant);
 ACO_API int aco_b200_get_ants(aco_b200_ctx *ctx, int *nodes /* m (n+2K) */,
                       int *lens /* m K */, double *cost, int *feasible,
                       int *steps, uint32_t *draws);

@@ -419,3 +419,37 @@ def test_setup_reuse_matches_fresh_contexts():
                 bn, bl, bc = reused.best()
                 fn, fl, fc = fresh.best()
                 assert bc == fc and np.array_equal(bn, fn) and np.array_equal(bl, fl)
+
+
+@pytest.mark.parametrize("n", [400, 1500, 3000])  # staged weights, packed levels, global rows
+def test_recorded_draws_match_reference_seq_code(oracle_mod, n):
+    """The harness of the parity contract: the GPU construction and the
+    reference's own build_ant_solution (src/seq/aco_sequential.c:616-681,
+    compiled from its sources) fed the same candidate lists, weights and an
+    arbitrary recorded stream of draws give the same routes."""
+    if not oracle_mod.ref_available():
+        pytest.skip("oracle/_ref not built")
+    O = oracle_mod
+    inst = I.uniform_instance(n, 6 + n // 500, 640 + n).unit_twin()
+    m, k = 16, 32
+    rs = np.random.RandomState(n)
+    draws = rs.randint(0, 1 << 24, size=(m, inst.n + inst.vehicles + 8)).astype(np.uint32)
+    with make_ctx(inst, k, m, seed=1) as ctx:
+        ctx.set_tau(random_tau(inst.n, 9 + n))
+        ctx.construct_with_draws(draws)
+        nodes, lens, cost, feas, steps, used = ctx.ants()
+        cand, lvl = ctx.candidates()
+        A, lut, _ = O.tables()
+        w = O.weights(inst.n, k, cand, lvl, ctx.tau(), A, lut)
+        for a in range(m):
+            rn, rl, rc, ru = O.ref_construct_ant(inst.x, inst.y, inst.vehicles, inst.capacity,
+                                                 k, cand, w, draws[a])
+            assert np.array_equal(lens[a], rl) and np.array_equal(nodes[a][: rl.sum()], rn)
+            assert abs(cost[a] - rc) <= 1e-9 * rc and used[a] == ru
+        # Philox draws recorded and replayed give the Philox run's routes
+        ctx.construct(3)
+        n1, l1, *_ = ctx.ants()
+        rec = np.stack([O.draws(1, 3, a, 0, inst.n + inst.vehicles + 8) for a in range(m)])
+        ctx.construct_with_draws(rec)
+        n2, l2, *_ = ctx.ants()
+        assert np.array_equal(n1, n2) and np.array_equal(l1, l2)

@@ -39,7 +39,7 @@ EXPORTED = [
     "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
     "aco_b200_batch_get", "aco_b200_batch_get_costs",
     "aco_b200_shard_packet_ints", "aco_b200_shard_construct", "aco_b200_shard_update",
-    "aco_b200_get_depot_tables", "aco_b200_debug_inject",
+    "aco_b200_get_depot_tables", "aco_b200_debug_inject", "aco_b200_construct_with_draws",
     "aco_b200_prior_create", "aco_b200_prior_destroy", "aco_b200_prior_set_stream",
     "aco_b200_prior_init", "aco_b200_prior_set_params", "aco_b200_prior_get_params",
     "aco_b200_prior_load", "aco_b200_prior_save", "aco_b200_prior_set_dataset",
@@ -139,6 +139,7 @@ def load():
         "aco_b200_shard_update": [vp, vp, i32],
         "aco_b200_get_depot_tables": [vp, vp, vp, vp],
         "aco_b200_debug_inject": [vp, i32, i32],
+        "aco_b200_construct_with_draws": [vp, vp, i32],
         "aco_b200_prior_create": [vp, i32], "aco_b200_prior_destroy": [vp],
         "aco_b200_prior_set_stream": [vp, vp], "aco_b200_prior_init": [vp, C.c_uint],
         "aco_b200_prior_set_params": [vp, vp, i32], "aco_b200_prior_get_params": [vp, vp, i32],
@@ -317,6 +318,13 @@ class Context:
         _check(self._lib.aco_b200_get_depot_tables(self._h, _p(lvl0), _p(rdep), C.byref(e)),
                "aco_b200_get_depot_tables")
         return lvl0, rdep, e.value
+
+    def construct_with_draws(self, draws) -> None:
+        """One construct pass on recorded draws [m][per_ant] (24-bit values)."""
+        d = np.ascontiguousarray(draws, np.uint32)
+        assert d.ndim == 2 and d.shape[0] == self.m
+        _check(self._lib.aco_b200_construct_with_draws(self._h, _p(d), d.shape[1]),
+               "aco_b200_construct_with_draws")
 
     def construct(self, epoch: int, layout: int = LAYOUT_AUTO) -> None:
         _check(self._lib.aco_b200_construct(self._h, epoch, layout), "aco_b200_construct")

@@ -167,7 +167,8 @@ cudaError_t launch_construct(const InstanceView &iv, const EpochTables &et,
                              const AntBuffers &ab, const SmemPlan &plan,
                              DevState *st, uint32_t seed, uint32_t epoch,
                              uint32_t stream_id, int use_state_epoch,
-                             cudaStream_t s);
+                             cudaStream_t s, const uint32_t *draw_src = nullptr,
+                             uint32_t draw_per_ant = 0);
 cudaError_t launch_best(const InstanceView &iv, const AntBuffers &ab,
                         DevState *st, int *gbest_nodes, int *gbest_lens,
                         EpochRec *log, cudaStream_t s);

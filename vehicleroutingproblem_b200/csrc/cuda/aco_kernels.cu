@@ -307,7 +307,28 @@ struct ConstructArgs {
   uint32_t epoch;
   uint32_t stream;
   int use_state_epoch;  // 1: epoch number = st->epoch (graph replays)
+  const uint32_t *draw_src;  // test hook: recorded draws [m][draw_per_ant], or null
+  uint32_t draw_per_ant;
 };
+
+// Next 128 draws of an ant: Philox, or (test hook) the recorded stream,
+// whose draws past its end read as 0.
+__device__ __forceinline__ void next_draws(const ConstructArgs &a, uint32_t *buf, uint32_t d,
+                                           uint32_t seed, uint32_t epoch, uint32_t gant,
+                                           int ant, int lane) {
+  if (a.draw_src) {
+    __syncwarp();
+    const uint32_t *src = a.draw_src + (size_t)ant * a.draw_per_ant;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t idx = (d & ~127u) + 4u * (uint32_t)lane + (uint32_t)q;
+      buf[4 * lane + q] = idx < a.draw_per_ant ? (src[idx] & 0xFFFFFFu) : 0u;
+    }
+    __syncwarp();
+    return;
+  }
+  draw_refill(buf, d, seed, epoch, gant, a.stream, lane);
+}
 
 // FP64 cost of a compact route sequence, summed in route order
 // (solution_cost, src/common/solution.c:126-137).  Lanes compute the arc
@@ -368,7 +389,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
   // split over several devices).
   const uint32_t gant = (uint32_t)(ant + iv.ant_base);
   uint32_t d = 0;
-  draw_refill(dbuf, d, seed, epoch, gant, a.stream, lane);
+  next_draws(a, dbuf, d, seed, epoch, gant, ant, lane);
   uint32_t r_next = dbuf[0];
 
   int remaining = iv.n;
@@ -432,10 +453,10 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       if (CREF && may_close) {
         if (denom == 0u) break;
         d += 1u;  // the roulette draw is spent
-        if ((d & 127u) == 0u) draw_refill(dbuf, d, seed, epoch, gant, a.stream, lane);
+        if ((d & 127u) == 0u) next_draws(a, dbuf, d, seed, epoch, gant, ant, lane);
         const uint32_t r2 = dbuf[d & 127u];
         d += 1u;  // and the close draw
-        if ((d & 127u) == 0u) draw_refill(dbuf, d, seed, epoch, gant, a.stream, lane);
+        if ((d & 127u) == 0u) next_draws(a, dbuf, d, seed, epoch, gant, ant, lane);
         r_next = dbuf[d & 127u];
         drawn = true;
         const double wd = depot_weight(a.et.rdep[cur], a.et.lut);
@@ -470,7 +491,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       if (!CREF || !drawn) {
         d += (denom != 0u) ? 1u : 0u;
         if ((d & 127u) == 0u && denom != 0u)
-          draw_refill(dbuf, d, seed, epoch, gant, a.stream, lane);
+          next_draws(a, dbuf, d, seed, epoch, gant, ant, lane);
         r_next = dbuf[d & 127u];
       }
     }
@@ -740,8 +761,11 @@ cudaError_t launch_construct(const InstanceView &iv, const EpochTables &et,
                              const AntBuffers &ab, const SmemPlan &plan,
                              DevState *st, uint32_t seed, uint32_t epoch,
                              uint32_t stream_id, int use_state_epoch,
-                             cudaStream_t s) {
+                             cudaStream_t s, const uint32_t *draw_src,
+                             uint32_t draw_per_ant) {
   ConstructArgs a;
+  a.draw_src = draw_src;
+  a.draw_per_ant = draw_per_ant;
   a.iv = iv;
   a.et = et;
   a.ab = ab;

@@ -866,6 +866,28 @@ int aco_b200_construct(aco_b200_ctx *ctx, int epoch, int layout) {
   return ACO_OK;
 }
 
+int aco_b200_construct_with_draws(aco_b200_ctx *ctx, const uint32_t *draws, int per_ant) {
+  if (!ctx || !ctx->ready || !draws || per_ant < 1) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(ctx->device);
+  PheromoneView pv = ctx->pv;
+  EpochTables et = ctx->et;
+  int rc = current_tau(ctx, &pv.tau);
+  if (rc) return rc;
+  et.tau_alt = nullptr;
+  const size_t bytes = (size_t)ctx->m * (size_t)per_ant * sizeof(uint32_t);
+  uint32_t *d = nullptr;
+  if (cudaMalloc(&d, bytes) != cudaSuccess) return ACO_ERR_ALLOCATION;
+  cudaError_t e = cudaMemcpyAsync(d, draws, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = launch_weights(ctx->iv, pv, et, nullptr, ctx->stream);
+  if (e == cudaSuccess)
+    e = launch_construct(ctx->iv, ctx->et, ctx->ab, ctx->plan, nullptr, ctx->seed, 0, 0, 0,
+                         ctx->stream, d, (uint32_t)per_ant);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  TRY(e);
+  return ACO_OK;
+}
+
 int aco_b200_get_ants(aco_b200_ctx *ctx, int *nodes, int *lens, double *cost,
                       int *feasible, int *steps, uint32_t *draws) {
   if (!ctx || !ctx->ready) return ACO_ERR_INVALID_INPUT;

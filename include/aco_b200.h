@@ -302,11 +302,19 @@ ACO_API int aco_b200_batch_autotune(aco_b200_batch *batch, int trial_epochs,
 ACO_API int aco_b200_batch_solve(aco_b200_batch *batch);
 ACO_API int aco_b200_batch_enqueue(aco_b200_batch *batch);
 ACO_API int aco_b200_batch_synchronize(aco_b200_batch *batch);
-/* Best solution of one instance (compact form, as aco_b200_get_best). */
+/* Results are read after the batch's stream (the solve included): every
+ * getter below copies on that stream and waits for it.
+ * Best solution of one instance (compact form, as aco_b200_get_best). */
 ACO_API int aco_b200_batch_get(aco_b200_batch *batch, int instance, int *nodes, int *lens,
                                double *cost, int *epochs);
 ACO_API int aco_b200_batch_get_costs(aco_b200_batch *batch, double *costs, int *epochs,
                                      unsigned long long *steps);
+/* Best solutions of every instance in three copies.  nodes: sum of
+ * n_i + 2 K_i ints, instance i's compact sequence at offset
+ * sum_{j<i} (n_j + 2 K_j) (its first sum(lens) entries are used);
+ * lens: sum of K_i ints, instance i's at sum_{j<i} K_j; costs: count doubles
+ * (DBL_MAX where no ant was feasible).  Any pointer may be NULL. */
+ACO_API int aco_b200_batch_get_all(aco_b200_batch *batch, int *nodes, int *lens, double *costs);
 /* Learned eta levels for every instance of the batch (after setup). */
 ACO_API int aco_b200_batch_apply_prior(aco_b200_batch *batch, aco_b200_prior *prior, float gamma);
 

@@ -75,3 +75,29 @@ def test_autotune_keeps_results():
         assert np.all(e1 == 6) and np.all(np.isfinite(c1) | (c1 > 1e300))
     for i in (0, 7, 23):
         assert plain(insts[i], 9 + i, 32, 16, 6)[2] == c1[i]
+
+
+def test_setup_reuse_and_get_all(reference_runs):
+    """One batch object solving a stream of batches: a smaller batch reuses
+    the device buffers, a larger one reallocates them; every solve equals a
+    fresh object's, and get_all returns what the per-instance getter does."""
+    insts, ref = reference_runs
+    small = insts[:3]
+    large = insts + I.batched_instances(6, seed0=31500)
+    with _native.Batch(0) as fresh:
+        fresh.setup(large, ants=16, cand_k=16, seed=500, epochs=12)
+        fresh.solve()
+        want_large = [fresh.best(i) for i in range(len(large))]
+    with _native.Batch(0) as b:
+        for batch in (insts, small, insts, large):
+            b.setup(batch, ants=16, cand_k=16, seed=500, epochs=12)
+            b.solve()
+            got = b.best_all()
+            assert len(got) == len(batch)
+            for i, (nodes, lens, cost) in enumerate(got):
+                one = b.best(i)
+                assert np.array_equal(nodes, one[0]) and np.array_equal(lens, one[1])
+                assert cost == one[2]
+                want = ref[i][:3] if batch is not large else want_large[i][:3]
+                assert cost == want[2], (i, cost, want[2])
+                assert np.array_equal(nodes, want[0]) and np.array_equal(lens, want[1])

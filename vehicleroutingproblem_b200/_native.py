@@ -37,7 +37,7 @@ EXPORTED = [
     "aco_b200_batch_set_stream",
     "aco_b200_batch_set_tuning", "aco_b200_batch_get_tuning", "aco_b200_batch_autotune",
     "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
-    "aco_b200_batch_get", "aco_b200_batch_get_costs",
+    "aco_b200_batch_get", "aco_b200_batch_get_costs", "aco_b200_batch_get_all",
     "aco_b200_shard_packet_ints", "aco_b200_shard_construct", "aco_b200_shard_update",
     "aco_b200_get_depot_tables", "aco_b200_debug_inject", "aco_b200_construct_with_draws",
     "aco_b200_prior_create", "aco_b200_prior_destroy", "aco_b200_prior_set_stream",
@@ -134,6 +134,7 @@ def load():
         "aco_b200_batch_solve": [vp], "aco_b200_batch_enqueue": [vp],
         "aco_b200_batch_synchronize": [vp],
         "aco_b200_batch_get": [vp, i32, vp, vp, vp, vp],
+        "aco_b200_batch_get_all": [vp, vp, vp, vp],
         "aco_b200_batch_get_costs": [vp, vp, vp, vp],
         "aco_b200_shard_packet_ints": [vp], "aco_b200_shard_construct": [vp, vp],
         "aco_b200_shard_update": [vp, vp, i32],
@@ -605,6 +606,30 @@ class Batch:
             return nodes[:0], lens, float("inf"), ep.value
         _check(rc, "aco_b200_batch_get")
         return nodes[: int(lens.sum())].copy(), lens, cost.value, ep.value
+
+    def best_all(self):
+        """Best solution of every instance, read in three copies: a list of
+        (nodes, lens, cost) as best() returns them (nodes empty and cost inf
+        where no ant was feasible)."""
+        insts = self.instances
+        slot = np.array([i.n + 2 * i.vehicles for i in insts], np.int64)
+        kv = np.array([i.vehicles for i in insts], np.int64)
+        nodes = np.zeros(int(slot.sum()), np.int32)
+        lens = np.zeros(int(kv.sum()), np.int32)
+        costs = np.zeros(len(insts), np.float64)
+        _check(self._lib.aco_b200_batch_get_all(self._h, _p(nodes), _p(lens), _p(costs)),
+               "aco_b200_batch_get_all")
+        out = []
+        no = np.concatenate([[0], np.cumsum(slot)])
+        lo = np.concatenate([[0], np.cumsum(kv)])
+        for i in range(len(insts)):
+            ln = lens[lo[i]:lo[i + 1]].copy()
+            c = float(costs[i])
+            if c >= np.finfo(np.float64).max:
+                out.append((nodes[:0].copy(), ln, float("inf")))
+            else:
+                out.append((nodes[no[i]:no[i] + int(ln.sum())].copy(), ln, c))
+        return out
 
     def apply_prior(self, prior: Optional[Prior], gamma: float = 1.0) -> None:
         _check(self._lib.aco_b200_batch_apply_prior(self._h, prior._h if prior else None, gamma),

@@ -319,14 +319,30 @@ __device__ void seg_build_ant(const BatchArgs &a, const BatchInst &I, const Seg<
   }
   sg.sync();
   // FP64 cost in route order (boundary (0,0) pairs add +0.0).
+  // The next LANES arcs' end points are loaded while the current ones are
+  // summed.
   double acc = 0.0;
   const int arcs = pos - 1;
+  int ru = 0, rv = 0;
+  if (sg.lane < arcs) {
+    ru = route[sg.lane];
+    rv = route[sg.lane + 1];
+  }
   for (int b = 0; b < arcs; b += LANES) {
-    const int j = b + sg.lane;
     double dj = 0.0;
-    if (j < arcs) dj = dist64(coords[route[j]], coords[route[j + 1]]);
-    const int cnt = (arcs - b < LANES) ? arcs - b : LANES;
-    for (int t = 0; t < cnt; ++t) acc = __dadd_rn(acc, sg.shfl(dj, t));
+    if (b + sg.lane < arcs) dj = dist64(coords[ru], coords[rv]);
+    const int j2 = b + LANES + sg.lane;
+    if (j2 < arcs) {
+      ru = route[j2];
+      rv = route[j2 + 1];
+    }
+    if (arcs - b >= LANES) {
+#pragma unroll
+      for (int t = 0; t < LANES; ++t) acc = __dadd_rn(acc, sg.shfl(dj, t));
+    } else {
+      const int cnt = arcs - b;
+      for (int t = 0; t < cnt; ++t) acc = __dadd_rn(acc, sg.shfl(dj, t));
+    }
   }
   if (sg.lane == 0) {
     a.cost[ai] = acc;
@@ -609,25 +625,29 @@ struct aco_b200_batch {
   BatchArgs args = {};
   std::vector<BatchInst> inst;
   std::vector<int> sizes;  // work estimate per instance
-  void *bufs[32] = {nullptr};
-  int nbufs = 0;
+  // Every device buffer is a 256-byte aligned slice of one allocation; a
+  // set-up reuses it while the new batch fits, so solving a stream of
+  // batches allocates once.
+  unsigned char *arena = nullptr;
+  size_t arena_cap = 0, arena_used = 0;
+  bool sizing = false;
   aco_b200_batch_tuning tuning = {32, 16, 1};
   const float *d_thr = nullptr;  // eta thresholds (plain levels)
+  const long long *d_seg_off = nullptr;  // first row of every instance
+  const int *d_seg_n = nullptr;          // customers of every instance
+  long long rows = 0;                    // sum of n + 1
   void free_all() {
-    for (int i = 0; i < nbufs; ++i) cudaFree(bufs[i]);
-    nbufs = 0;
+    if (arena) cudaFree(arena);
+    arena = nullptr;
+    arena_cap = arena_used = 0;
     ready = false;
   }
   template <typename T>
-  cudaError_t alloc(T **p, size_t count) {
+  void carve(T **p, size_t count) {
     size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
     if (bytes == 0) bytes = 256;
-    cudaError_t e = cudaMalloc((void **)p, bytes);
-    if (e == cudaSuccess) {
-      bufs[nbufs++] = *p;
-      e = cudaMemset(*p, 0, bytes);
-    }
-    return e;
+    *p = sizing ? nullptr : reinterpret_cast<T *>(arena + arena_used);
+    arena_used += bytes;
   }
 };
 
@@ -702,7 +722,7 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
   if (!b || !p || p->count <= 0 || !p->n || !p->K || !p->capacity || !p->x || !p->y)
     return ACO_ERR_INVALID_INPUT;
   cudaSetDevice(b->device);
-  b->free_all();
+  b->ready = false;
   const int count = p->count;
   int k = p->cand_k > 0 ? p->cand_k : 32;
   if (k > kMaxCand) k = kMaxCand;
@@ -713,6 +733,8 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
   int max_rows = 0, max_K = 0, max_n = 0;
   std::vector<float2> xy;
   std::vector<int> dem;
+  std::vector<long long> seg_off(count);
+  std::vector<int> seg_n(count);
   for (int i = 0; i < count; ++i) {
     const int n = p->n[i], K = p->K[i];
     const long long cap = p->capacity[i];
@@ -744,6 +766,8 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
     I.max_demand = mx;
     I.unit = unit ? 1 : 0;
     I.node_off = node;
+    seg_off[i] = node;
+    seg_n[i] = n;
     I.tau_off = taub;
     I.route_off = route;
     I.lens_off = lensn;
@@ -819,40 +843,62 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
   int32_t *d_A;
   uint32_t *d_lut;
   float *d_thr;
-  BTRY(b->alloc(&d_inst, count));
-  BTRY(b->alloc(&d_order, count));
-  BTRY(b->alloc(&d_coords, node));
-  BTRY(b->alloc(&d_dem, node));
-  BTRY(b->alloc(&d_cand, node * k));
-  BTRY(b->alloc(&d_lvl, node * k));
-  BTRY(b->alloc(&d_A, 256));
-  BTRY(b->alloc(&d_lut, 256));
-  BTRY(b->alloc(&d_thr, kThresholds));
-  BTRY(b->alloc(&a.tau, taub));
-  BTRY(b->alloc(&a.routes, route));
-  BTRY(b->alloc(&a.lens, lensn));
-  BTRY(b->alloc(&a.loads, lensn));
-  BTRY(b->alloc(&a.repc, lensn));
-  BTRY(b->alloc(&a.rep, rep));
-  BTRY(b->alloc(&a.cost, (long long)count * m));
-  BTRY(b->alloc(&a.feasible, (long long)count * m));
-  BTRY(b->alloc(&a.steps, (long long)count * m));
-  BTRY(b->alloc(&a.gbest_nodes, gb));
-  BTRY(b->alloc(&a.gbest_lens, gbl));
-  BTRY(b->alloc(&a.out_cost, count));
-  BTRY(b->alloc(&a.out_epochs, count));
-  BTRY(b->alloc(&a.out_steps, count));
-  BTRY(b->alloc(&a.queue, 1));
+  long long *d_soff;
+  int *d_sn;
+  auto layout = [&]() {
+    b->arena_used = 0;
+    b->carve(&d_inst, count);
+    b->carve(&d_order, count);
+    b->carve(&d_coords, node);
+    b->carve(&d_dem, node);
+    b->carve(&d_cand, node * k);
+    b->carve(&d_lvl, node * k);
+    b->carve(&d_A, 256);
+    b->carve(&d_lut, 256);
+    b->carve(&d_thr, kThresholds);
+    b->carve(&d_soff, count);
+    b->carve(&d_sn, count);
+    b->carve(&a.tau, taub);
+    b->carve(&a.routes, route);
+    b->carve(&a.lens, lensn);
+    b->carve(&a.loads, lensn);
+    b->carve(&a.repc, lensn);
+    b->carve(&a.rep, rep);
+    b->carve(&a.cost, (long long)count * m);
+    b->carve(&a.feasible, (long long)count * m);
+    b->carve(&a.steps, (long long)count * m);
+    b->carve(&a.gbest_nodes, gb);
+    b->carve(&a.gbest_lens, gbl);
+    b->carve(&a.out_cost, count);
+    b->carve(&a.out_epochs, count);
+    b->carve(&a.out_steps, count);
+    b->carve(&a.queue, 1);
+  };
+  b->sizing = true;
+  layout();
+  b->sizing = false;
+  const size_t need = b->arena_used;
+  if (need > b->arena_cap) {
+    b->free_all();
+    BTRY(cudaMalloc((void **)&b->arena, need));
+    b->arena_cap = need;
+  }
+  layout();
   cudaStream_t s = b->stream;
+  BTRY(cudaMemsetAsync(b->arena, 0, need, s));
   BTRY(cudaMemcpyAsync(d_inst, b->inst.data(), sizeof(BatchInst) * count, cudaMemcpyHostToDevice, s));
   BTRY(cudaMemcpyAsync(d_coords, xy.data(), sizeof(float2) * node, cudaMemcpyHostToDevice, s));
   BTRY(cudaMemcpyAsync(d_dem, dem.data(), sizeof(int) * node, cudaMemcpyHostToDevice, s));
   BTRY(cudaMemcpyAsync(d_A, A.data(), 1024, cudaMemcpyHostToDevice, s));
   BTRY(cudaMemcpyAsync(d_lut, lut.data(), 1024, cudaMemcpyHostToDevice, s));
   BTRY(cudaMemcpyAsync(d_thr, thr.data(), sizeof(float) * kThresholds, cudaMemcpyHostToDevice, s));
-  for (int i = 0; i < count; ++i)
-    BTRY(launch_knn_levels(d_coords + b->inst[i].node_off, b->inst[i].n, k, d_thr, kThresholds,
-                           d_cand + b->inst[i].node_off * k, d_lvl + b->inst[i].node_off * k, s));
+  BTRY(cudaMemcpyAsync(d_soff, seg_off.data(), sizeof(long long) * count, cudaMemcpyHostToDevice, s));
+  BTRY(cudaMemcpyAsync(d_sn, seg_n.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s));
+  BTRY(launch_knn_levels_multi(d_coords, d_soff, d_sn, count, node, k, d_thr, kThresholds, d_cand,
+                               d_lvl, s));
+  b->d_seg_off = d_soff;
+  b->d_seg_n = d_sn;
+  b->rows = node;
   b->d_thr = d_thr;
   a.inst = d_inst;
   a.order = d_order;
@@ -885,8 +931,10 @@ int aco_b200_batch_set_tuning(aco_b200_batch *b, const aco_b200_batch_tuning *t)
     std::stable_sort(order.begin(), order.end(),
                      [&](int x, int y) { return b->sizes[x] > b->sizes[y]; });
   cudaSetDevice(b->device);
-  BTRY(cudaMemcpy(const_cast<int *>(b->args.order), order.data(), sizeof(int) * b->count,
-                  cudaMemcpyHostToDevice));
+  // Stream-ordered after any solve in flight; a pageable source is staged
+  // before the call returns.
+  BTRY(cudaMemcpyAsync(const_cast<int *>(b->args.order), order.data(), sizeof(int) * b->count,
+                       cudaMemcpyHostToDevice, b->stream));
   b->tuning = *t;
   return ACO_OK;
 }
@@ -975,12 +1023,17 @@ int aco_b200_batch_get(aco_b200_batch *b, int instance, int *nodes, int *lens, d
   if (!b || !b->ready || instance < 0 || instance >= b->count) return ACO_ERR_INVALID_INPUT;
   cudaSetDevice(b->device);
   const BatchInst &I = b->inst[instance];
-  BTRY(cudaMemcpy(cost, b->args.out_cost + instance, sizeof(double), cudaMemcpyDeviceToHost));
-  if (epochs) BTRY(cudaMemcpy(epochs, b->args.out_epochs + instance, sizeof(int), cudaMemcpyDeviceToHost));
-  if (lens) BTRY(cudaMemcpy(lens, b->args.gbest_lens + I.gblens_off, sizeof(int) * I.K, cudaMemcpyDeviceToHost));
+  cudaStream_t s = b->stream;
+  BTRY(cudaMemcpyAsync(cost, b->args.out_cost + instance, sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (epochs)
+    BTRY(cudaMemcpyAsync(epochs, b->args.out_epochs + instance, sizeof(int), cudaMemcpyDeviceToHost, s));
+  if (lens)
+    BTRY(cudaMemcpyAsync(lens, b->args.gbest_lens + I.gblens_off, sizeof(int) * I.K,
+                         cudaMemcpyDeviceToHost, s));
   if (nodes)
-    BTRY(cudaMemcpy(nodes, b->args.gbest_nodes + I.gbest_off, sizeof(int) * (I.n + 2 * I.K),
-                    cudaMemcpyDeviceToHost));
+    BTRY(cudaMemcpyAsync(nodes, b->args.gbest_nodes + I.gbest_off, sizeof(int) * (I.n + 2 * I.K),
+                         cudaMemcpyDeviceToHost, s));
+  BTRY(cudaStreamSynchronize(s));
   return *cost < DBL_MAX ? ACO_OK : ACO_ERR_NO_SOLUTION;
 }
 
@@ -988,11 +1041,33 @@ int aco_b200_batch_get_costs(aco_b200_batch *b, double *costs, int *epochs,
                              unsigned long long *steps) {
   if (!b || !b->ready) return ACO_ERR_INVALID_INPUT;
   cudaSetDevice(b->device);
-  if (costs) BTRY(cudaMemcpy(costs, b->args.out_cost, sizeof(double) * b->count, cudaMemcpyDeviceToHost));
-  if (epochs) BTRY(cudaMemcpy(epochs, b->args.out_epochs, sizeof(int) * b->count, cudaMemcpyDeviceToHost));
+  cudaStream_t s = b->stream;
+  if (costs)
+    BTRY(cudaMemcpyAsync(costs, b->args.out_cost, sizeof(double) * b->count, cudaMemcpyDeviceToHost, s));
+  if (epochs)
+    BTRY(cudaMemcpyAsync(epochs, b->args.out_epochs, sizeof(int) * b->count, cudaMemcpyDeviceToHost, s));
   if (steps)
-    BTRY(cudaMemcpy(steps, b->args.out_steps, sizeof(unsigned long long) * b->count,
-                    cudaMemcpyDeviceToHost));
+    BTRY(cudaMemcpyAsync(steps, b->args.out_steps, sizeof(unsigned long long) * b->count,
+                         cudaMemcpyDeviceToHost, s));
+  BTRY(cudaStreamSynchronize(s));
+  return ACO_OK;
+}
+
+int aco_b200_batch_get_all(aco_b200_batch *b, int *nodes, int *lens, double *costs) {
+  if (!b || !b->ready) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(b->device);
+  cudaStream_t s = b->stream;
+  const BatchInst &last = b->inst[b->count - 1];
+  if (nodes)
+    BTRY(cudaMemcpyAsync(nodes, b->args.gbest_nodes,
+                         sizeof(int) * (last.gbest_off + last.n + 2 * last.K),
+                         cudaMemcpyDeviceToHost, s));
+  if (lens)
+    BTRY(cudaMemcpyAsync(lens, b->args.gbest_lens, sizeof(int) * (last.gblens_off + last.K),
+                         cudaMemcpyDeviceToHost, s));
+  if (costs)
+    BTRY(cudaMemcpyAsync(costs, b->args.out_cost, sizeof(double) * b->count, cudaMemcpyDeviceToHost, s));
+  BTRY(cudaStreamSynchronize(s));
   return ACO_OK;
 }
 
@@ -1004,18 +1079,17 @@ extern "C" int aco_b200_batch_apply_prior(aco_b200_batch *b, aco_b200_prior *pri
   cudaStream_t s = b->stream;
   const BatchArgs &a = b->args;
   uint16_t *lvl = const_cast<uint16_t *>(a.lvl);
-  for (int i = 0; i < b->count; ++i) {
-    const BatchInst &I = b->inst[i];
-    if (prior && gamma > 0.f) {
+  if (prior && gamma > 0.f) {
+    for (int i = 0; i < b->count; ++i) {
+      const BatchInst &I = b->inst[i];
       int rc = acob200::prior::learned_levels(prior, a.coords + I.node_off, a.demand + I.node_off,
                                               I.cap, I.n, b->k, a.cand + I.node_off * b->k,
                                               lvl + I.node_off * b->k, gamma, 0, s);
       if (rc) return rc;
-    } else {
-      BTRY(launch_knn_levels(a.coords + I.node_off, I.n, b->k, b->d_thr, kThresholds,
-                             const_cast<uint16_t *>(a.cand) + I.node_off * b->k,
-                             lvl + I.node_off * b->k, s));
     }
+  } else {
+    BTRY(launch_knn_levels_multi(a.coords, b->d_seg_off, b->d_seg_n, b->count, b->rows, b->k,
+                                 b->d_thr, kThresholds, const_cast<uint16_t *>(a.cand), lvl, s));
   }
   BTRY(cudaStreamSynchronize(s));
   return ACO_OK;

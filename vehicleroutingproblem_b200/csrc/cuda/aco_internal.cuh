@@ -159,6 +159,12 @@ struct PheromoneView {
 cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
                               const float *thr, int J, uint16_t *cand,
                               uint16_t *lvl, cudaStream_t s);
+// Candidate lists of `count` instances packed one after another: instance s
+// has seg_n[s] customers and starts at row seg_off[s] (device arrays).
+cudaError_t launch_knn_levels_multi(const float2 *coords, const long long *seg_off,
+                                    const int *seg_n, int count, long long rows, int k,
+                                    const float *thr, int J, uint16_t *cand, uint16_t *lvl,
+                                    cudaStream_t s);
 cudaError_t launch_fill_u8(uint8_t *p, unsigned long long count, uint8_t v,
                            cudaStream_t s);
 cudaError_t launch_weights(const InstanceView &iv, const PheromoneView &pv,

@@ -63,6 +63,50 @@ cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
   return cudaGetLastError();
 }
 
+// Candidate lists of many instances in one launch.  Instance s owns rows
+// [seg_off[s], seg_off[s] + seg_n[s] + 1) of the concatenated coordinates
+// (seg_off ascending); each warp finds its row's instance by binary search and
+// writes the same lists as k_knn_levels on that instance alone.
+__global__ void __launch_bounds__(256) k_knn_levels_multi(
+    const float2 *__restrict__ coords, const long long *__restrict__ seg_off,
+    const int *__restrict__ seg_n, int count, long long rows, int k,
+    const float *__restrict__ thr, int J, uint16_t *__restrict__ cand,
+    uint16_t *__restrict__ lvl) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  for (long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows;
+       r += warps) {
+    int lo = 0, hi = count;  // last s with seg_off[s] <= r
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(seg_off + mid) <= r) lo = mid; else hi = mid;
+    }
+    const long long off = __ldg(seg_off + lo);
+    const int n = __ldg(seg_n + lo);
+    const int i = (int)(r - off);
+    if (i > n) continue;  // gap rows (none when the segments are packed)
+    const unsigned long long key = warp_knn(coords + off, n, k, i, lane);
+    if (lane < k) {
+      const int node = (key == ~0ull) ? 0 : (int)(key & 0xffffffffu);
+      const float d2 = __uint_as_float((unsigned)(key >> 32));
+      cand[(size_t)r * k + lane] = (uint16_t)node;
+      lvl[(size_t)r * k + lane] = (uint16_t)(node ? level_of(d2, thr, J) : 0);
+    }
+  }
+}
+
+cudaError_t launch_knn_levels_multi(const float2 *coords, const long long *seg_off,
+                                    const int *seg_n, int count, long long rows, int k,
+                                    const float *thr, int J, uint16_t *cand, uint16_t *lvl,
+                                    cudaStream_t s) {
+  if (count < 1 || rows < 1) return cudaErrorInvalidValue;
+  long long blocks = (rows + 7) / 8;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_knn_levels_multi<<<(int)blocks, 256, 0, s>>>(coords, seg_off, seg_n, count, rows, k, thr, J,
+                                                 cand, lvl);
+  return cudaGetLastError();
+}
+
 // eta level of d(i,0)^2 for every node (reference-CUDA depot rule).
 __global__ void k_depot_levels(const float2 *__restrict__ coords, int n,
                                const float *__restrict__ thr, int J, uint16_t *lvl0) {
@@ -340,12 +384,27 @@ __device__ __forceinline__ double route_cost(const Tables<L, UNIT> &tb,
                                              int lane) {
   double acc = 0.0;
   const int arcs = entries - 1;
+  // The next 32 arcs' end points are loaded while the current ones are summed.
+  int u = 0, v = 0;
+  if (lane < arcs) {
+    u = route[lane];
+    v = route[lane + 1];
+  }
   for (int b = 0; b < arcs; b += 32) {
-    const int j = b + lane;
     double dj = 0.0;
-    if (j < arcs) dj = dist64(tb.coord(route[j]), tb.coord(route[j + 1]));
-    const int cnt = (arcs - b < 32) ? arcs - b : 32;
-    for (int t = 0; t < cnt; ++t) acc = __dadd_rn(acc, __shfl_sync(kFull, dj, t));
+    if (b + lane < arcs) dj = dist64(tb.coord(u), tb.coord(v));
+    const int j2 = b + 32 + lane;
+    if (j2 < arcs) {
+      u = route[j2];
+      v = route[j2 + 1];
+    }
+    if (arcs - b >= 32) {
+#pragma unroll
+      for (int t = 0; t < 32; ++t) acc = __dadd_rn(acc, __shfl_sync(kFull, dj, t));
+    } else {
+      const int cnt = arcs - b;
+      for (int t = 0; t < cnt; ++t) acc = __dadd_rn(acc, __shfl_sync(kFull, dj, t));
+    }
   }
   return acc;
 }

@@ -463,8 +463,9 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
     int load = 0;
     const long long fut64 = (long long)(K - v - 1) * iv.cap;
     const int future = fut64 > 0x7fffffffLL ? 0x7fffffff : (int)fut64;
-    int room = cap;
-    bool tight = !UNIT && room < max_dem;
+    // room < max_dem  <=>  load > cap - max_dem
+    const int tight_load = cap - max_dem;
+    bool tight = !UNIT && 0 > tight_load;
     // Row of the current node; the next row's loads are issued as soon as the
     // next node is known, ahead of this step's bookkeeping.
     int c = 0, dc = 0;
@@ -482,7 +483,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       bool ok = !vis.test(c);
       // Demands only bind when the room left is below the largest demand;
       // until then the speculative demand load stays off the step's chain.
-      if (!UNIT && tight) ok = ok && dc <= room;
+      if (!UNIT && tight) ok = ok && dc + load <= cap;
       const uint32_t wv = ok ? w : 0u;
       const uint32_t denom = __reduce_add_sync(kFull, wv);
       // cum * 2^24 >= r * denom  <=>  cum >= ceil(r * denom / 2^24)
@@ -505,7 +506,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
         }
         msk = __ballot_sync(kFull, wv != 0u && cum >= thr);
       }
-      const int src = msk ? __ffs(msk) - 1 : 0;
+      const int src = __ffs(msk) - 1;  // -1 (lane 31) only when denom == 0
       int next = __shfl_sync(kFull, c, src);
       int dn = UNIT ? 1 : __shfl_sync(kFull, dc, src);
       bool drawn = false;  // draws of this step already accounted
@@ -523,7 +524,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
           break;
       }
       if (denom == 0u) {
-        next = nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), room, tight, lane);
+        next = nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), cap - load, tight, lane);
         if (next <= 0) break;
         dn = tb.demand(next);
       }
@@ -543,8 +544,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       --remaining;
       load += dn;
       rem_dem -= dn;
-      room = cap - load;
-      tight = !UNIT && room < max_dem;
+      tight = !UNIT && load > tight_load;
       cur = next;
       // A draw is consumed only by a roulette selection (denom > 0).
       if (!CREF || !drawn) {

@@ -295,15 +295,16 @@ struct Visited {
     return word;
   }
   __device__ __forceinline__ bool test(int c) const {
-    return (word_of(c) & (1u << (c & 31))) != 0u;
+    const uint32_t word = word_of(c);
+    return (__funnelshift_r(word, word, c) & 1u) != 0u;  // bit c mod 32
   }
   __device__ __forceinline__ void set(int node, int lane) {
-    const uint32_t bit = 1u << (node & 31);
+    const uint32_t bit = __funnelshift_l(0u, 1u, node);  // 1 << (node mod 32)
     if (V == 0) {
       if (lane == 0) s[node >> 5] |= bit;
       __syncwarp();
     } else {
-      const bool mine = lane == ((node >> 5) & 31);
+      const bool mine = lane == (V == 1 ? (node >> 5) : ((node >> 5) & 31));
       if (V == 2 && (node >> 10)) w1 |= mine ? bit : 0u;
       else w0 |= mine ? bit : 0u;
     }
@@ -477,6 +478,26 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
     if (!UNIT) dc = tb.demand(c);
     // Every demand is >= 1, so rem_dem > future >= 0 implies remaining > 0.
     const int limit = CREF ? 0 : future;
+    // One step to customer nx of demand dnx: the next row's loads first,
+    // then the bookkeeping.
+    auto take_step = [&](int nx, int dnx) {
+      const int base = nx * k;
+      c = 0;
+      w = 0u;
+      if (lane < k) {
+        c = tb.cand[base + lane];
+        w = tb.weight(base + lane);
+      }
+      if (!UNIT) dc = tb.demand(c);
+      route[pos] = nx;  // every lane stores the same value
+      vis.set(nx, lane);
+      ++pos;
+      --remaining;
+      load += dnx;
+      rem_dem -= dnx;
+      tight = !UNIT && load > tight_load;
+      cur = nx;
+    };
     while (rem_dem > limit && load < cap) {
       const bool may_close = CREF && rem_dem <= future;
       if (CREF && may_close && cur == 0) break;
@@ -505,13 +526,23 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
           if (lane >= o) cum += t;
         }
         msk = __ballot_sync(kFull, wv != 0u && cum >= thr);
+        if (denom == 0u) {
+          // No eligible candidate: the reference-CUDA rule closes the route
+          // when it may; otherwise the nearest eligible customer, which
+          // consumes no draw.
+          if (CREF && may_close) break;
+          const int nx = nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), cap - load,
+                                                       tight, lane);
+          if (nx <= 0) break;
+          take_step(nx, tb.demand(nx));
+          continue;
+        }
       }
       const int src = __ffs(msk) - 1;  // -1 (lane 31) only when denom == 0
       int next = __shfl_sync(kFull, c, src);
       int dn = UNIT ? 1 : __shfl_sync(kFull, dc, src);
       bool drawn = false;  // draws of this step already accounted
       if (CREF && may_close) {
-        if (denom == 0u) break;
         d += 1u;  // the roulette draw is spent
         if ((d & 127u) == 0u) next_draws(a, dbuf, d, seed, epoch, gant, ant, lane);
         const uint32_t r2 = dbuf[d & 127u];
@@ -523,34 +554,11 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
         if (__dmul_rn((double)r2, __dadd_rn((double)denom, wd)) >= (double)denom * 16777216.0)
           break;
       }
-      if (denom == 0u) {
-        next = nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), cap - load, tight, lane);
-        if (next <= 0) break;
-        dn = tb.demand(next);
-      }
-      {
-        const int base = next * k;
-        c = 0;
-        w = 0u;
-        if (lane < k) {
-          c = tb.cand[base + lane];
-          w = tb.weight(base + lane);
-        }
-        if (!UNIT) dc = tb.demand(c);
-      }
-      route[pos] = next;  // every lane stores the same value
-      vis.set(next, lane);
-      ++pos;
-      --remaining;
-      load += dn;
-      rem_dem -= dn;
-      tight = !UNIT && load > tight_load;
-      cur = next;
+      take_step(next, dn);
       // A draw is consumed only by a roulette selection (denom > 0).
-      if (!CREF || !drawn) {
-        d += (denom != 0u) ? 1u : 0u;
-        if ((d & 127u) == 0u && denom != 0u)
-          next_draws(a, dbuf, d, seed, epoch, gant, ant, lane);
+      if (!drawn) {
+        d += 1u;
+        if ((d & 127u) == 0u) next_draws(a, dbuf, d, seed, epoch, gant, ant, lane);
         r_next = dbuf[d & 127u];
       }
     }

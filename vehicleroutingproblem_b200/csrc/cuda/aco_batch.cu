@@ -147,11 +147,11 @@ struct SegVisited {
       const uint32_t hi = sg.shfl(w1, wi & (LANES - 1));
       word = (wi >= LANES) ? hi : word;
     }
-    return (word >> (c & 31)) & 1u;
+    return __funnelshift_r(word, word, c) & 1u;  // bit c mod 32
   }
   __device__ __forceinline__ void set(const Seg<LANES> &sg, int node) {
     const int wi = node >> 5;
-    const uint32_t bit = 1u << (node & 31);
+    const uint32_t bit = __funnelshift_l(0u, 1u, node);  // 1 << (node mod 32)
     if (sg.lane == (wi & (LANES - 1))) {
       if (V == 2 && wi >= LANES) w1 |= bit; else w0 |= bit;
     }
@@ -200,14 +200,14 @@ __device__ __forceinline__ void seg_draw_refill(uint32_t *buf, uint32_t d, uint3
 
 // One ant on one segment: the rules of build_ant in aco_kernels.cu
 // (src/seq/aco_sequential.c:616-681 with the demand extension), on the
-// block's shared tables.
-template <int LANES, int V>
+// block's shared tables.  UNIT: every customer's demand is 1 (instance flag).
+template <int LANES, int V, bool UNIT>
 __device__ void seg_build_ant(const BatchArgs &a, const BatchInst &I, const Seg<LANES> &sg,
                               const uint16_t *cand, const uint32_t *wt, const float2 *coords,
                               const int *dem, uint32_t *dbuf, uint32_t seed, int ant,
                               uint32_t epoch, long long ai) {
   const int k = a.k, K = I.K, n = I.n, R = n + 2 * K, cap = I.cap;
-  const bool unit = I.unit != 0;
+  constexpr bool unit = UNIT;
   int *route = a.routes + I.route_off + (long long)ant * R;
   int *lens = a.lens + I.lens_off + (long long)ant * K;
   int *loads = a.loads + I.lens_off + (long long)ant * K;
@@ -217,6 +217,7 @@ __device__ void seg_build_ant(const BatchArgs &a, const BatchInst &I, const Seg<
   seg_draw_refill(dbuf, d, seed, epoch, (uint32_t)ant, sg.lane, LANES, sg.mask);
   uint32_t r_next = dbuf[0];
   int remaining = n, rem_dem = I.total_demand, pos = 0;
+  const int tight_load = cap - I.max_demand;
   for (int v = 0; v < K; ++v) {
     const int start = pos;
     route[pos] = 0;
@@ -225,8 +226,8 @@ __device__ void seg_build_ant(const BatchArgs &a, const BatchInst &I, const Seg<
     const long long fut64 = (long long)(K - v - 1) * cap;
     const int future = fut64 > 0x7fffffffLL ? 0x7fffffff : (int)fut64;
     while (rem_dem > future && load < cap) {
-      const int room = cap - load;
-      const bool tight = !unit && room < I.max_demand;
+      // room < max demand  <=>  load > cap - max demand
+      const bool tight = !unit && load > tight_load;
       int c = 0;
       uint32_t w = 0u;
       if (sg.lane < k) {
@@ -234,7 +235,7 @@ __device__ void seg_build_ant(const BatchArgs &a, const BatchInst &I, const Seg<
         w = wt[cur * k + sg.lane];
       }
       bool ok = !vis.test(sg, c);
-      if (tight) ok = ok && dem[c] <= room;
+      if (tight) ok = ok && dem[c] + load <= cap;
       const uint32_t wv = ok ? w : 0u;
       const uint32_t denom = sg.sum(wv);
       uint32_t cum = wv;
@@ -248,12 +249,12 @@ __device__ void seg_build_ant(const BatchArgs &a, const BatchInst &I, const Seg<
         const uint32_t thr =
             (uint32_t)(((unsigned long long)r_next * denom + 0xFFFFFFull) >> kDrawBits);
         const unsigned msk = sg.ballot(wv != 0u && cum >= thr);
-        next = sg.shfl(c, msk ? __ffs(msk) - 1 : 0);
+        next = sg.shfl(c, __ffs(msk) - 1);  // msk != 0 when denom != 0
         ++d;
         if ((d & 127u) == 0u) seg_draw_refill(dbuf, d, seed, epoch, (uint32_t)ant, sg.lane, LANES, sg.mask);
         r_next = dbuf[d & 127u];
       } else {
-        next = seg_nearest<LANES, V>(sg, vis, coords, dem, unit, coords[cur], room, tight);
+        next = seg_nearest<LANES, V>(sg, vis, coords, dem, unit, coords[cur], cap - load, tight);
         if (next <= 0) break;
       }
       route[pos] = next;
@@ -450,8 +451,13 @@ __global__ void __launch_bounds__(1024) k_batch_solve(BatchArgs a, BatchSmem ly,
         const int ant = a0 + seg;
         if (seg < ants_per_block && ant < a.m) {
           const long long ai = (long long)ii * a.m + ant;
-          if (V == 1) seg_build_ant<LANES, 1>(a, I, sg, s_cand, s_w, s_coords, s_dem, dbuf, seed, ant, (uint32_t)epoch, ai);
-          else seg_build_ant<LANES, 2>(a, I, sg, s_cand, s_w, s_coords, s_dem, dbuf, seed, ant, (uint32_t)epoch, ai);
+          if (I.unit) {
+            if (V == 1) seg_build_ant<LANES, 1, true>(a, I, sg, s_cand, s_w, s_coords, s_dem, dbuf, seed, ant, (uint32_t)epoch, ai);
+            else seg_build_ant<LANES, 2, true>(a, I, sg, s_cand, s_w, s_coords, s_dem, dbuf, seed, ant, (uint32_t)epoch, ai);
+          } else {
+            if (V == 1) seg_build_ant<LANES, 1, false>(a, I, sg, s_cand, s_w, s_coords, s_dem, dbuf, seed, ant, (uint32_t)epoch, ai);
+            else seg_build_ant<LANES, 2, false>(a, I, sg, s_cand, s_w, s_coords, s_dem, dbuf, seed, ant, (uint32_t)epoch, ai);
+          }
         }
       }
       __syncthreads();

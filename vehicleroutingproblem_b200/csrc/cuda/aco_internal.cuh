@@ -433,9 +433,12 @@ __device__ __forceinline__ void deposit_arc(const PheromoneView &pv,
 template <class Nodes>
 __device__ void deposit_solution(const PheromoneView &pv, size_t stride,
                                  const Nodes &nodes, const int *lens, int K,
-                                 float dep, int *s_off) {
-  const int bd = (int)blockDim.x, tid = (int)threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5;
+                                 float dep, int *s_off, int gtid = 0, int gthreads = 0) {
+  // Arcs are shared out over gthreads threads (this thread is gtid) when
+  // several blocks deposit one solution, else over the block.
+  const int bd = gthreads > 0 ? gthreads : (int)blockDim.x;
+  const int tid = gthreads > 0 ? gtid : (int)threadIdx.x;
+  const int lane = (int)threadIdx.x & 31, warp = (int)threadIdx.x >> 5;
   if (!s_off) {
     int off = 0, base = 0;
     for (int v = 0; v < K; ++v) {

@@ -10,12 +10,16 @@
 //                     path's rules (src/seq/aco_sequential.c:477-681) over
 //                     candidate tables staged in shared memory by the TMA
 //                     engine (reference kernel: aco_cuda_kernels.cu:447-562)
-//   k_best            iteration best, global best and stop rules on the
+//   k_best_cluster    iteration best, global best, stop rules and both
+//                     deposits of the pipelined epoch over a cluster of 8
+//                     blocks; k_best the same without the deposits, on the
 //                     device (src/cuda/aco_cuda.cu:83-126, :331-399)
 //   k_evap_deposit    128-bit streaming evaporation, then the deposit of the
 //                     iteration best and global best by the last block
 //                     (aco_cuda_kernels.cu:145-155, :569-668)
 #include "aco_internal.cuh"
+
+#include <cooperative_groups.h>
 
 #include <cfloat>
 #include <climits>
@@ -904,7 +908,7 @@ __device__ int epoch_bookkeeping(DevState *st, bool found, double bc, int ba,
   rec.found = found ? 1 : 0;
   rec.global_best = st->global_best;
   rec.elapsed_ns = elapsed;
-  log[st->log_count % kLogCap] = rec;
+  if (log) log[st->log_count % kLogCap] = rec;
   st->log_count += 1;
   int flags = st->stop_flags;
   if (st->stagnation > 0 && st->iter_since_best >= st->stagnation) flags |= kStopStagnation;
@@ -915,19 +919,31 @@ __device__ int epoch_bookkeeping(DevState *st, bool found, double bc, int ba,
   return improved;
 }
 
+// The device state staged in shared memory by one block: one coalesced read,
+// the bookkeeping on the copy, one write-back before the block ends.
+__device__ __forceinline__ void state_load(DevState *s, const DevState *g) {
+  static_assert(sizeof(DevState) % sizeof(int) == 0, "DevState is whole words");
+  constexpr int kWords = (int)(sizeof(DevState) / sizeof(int));
+  for (int i = threadIdx.x; i < kWords; i += blockDim.x)
+    reinterpret_cast<int *>(s)[i] = reinterpret_cast<const volatile int *>(g)[i];
+  __syncthreads();
+}
+__device__ __forceinline__ void state_store(DevState *g, const DevState *s) {
+  constexpr int kWords = (int)(sizeof(DevState) / sizeof(int));
+  for (int i = threadIdx.x; i < kWords; i += blockDim.x)
+    reinterpret_cast<int *>(g)[i] = reinterpret_cast<const int *>(s)[i];
+}
+
 __device__ __forceinline__ uint32_t evap4(uint32_t x, uint32_t floor4,
                                           uint32_t delta4) {
   return __vsub4(__vmaxu4(x, floor4), delta4);
 }
 
-// DEPOSIT: the pipelined epoch -- the evaporated matrix already sits in the
-// other pheromone buffer; this block deposits the iteration best and the
-// global best there and makes it the current buffer.
-template <bool DEPOSIT>
-__global__ void __launch_bounds__(1024) k_best_t(InstanceView iv, AntBuffers ab,
-                                                 DevState *st, int *gbest_nodes,
-                                                 int *gbest_lens, EpochRec *log,
-                                                 PheromoneView pv, uint8_t *tau_alt) {
+// Iteration best, bookkeeping and the global-best copy in one block, for the
+// epochs whose pheromone update is a separate k_evap_deposit launch.
+__global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
+                                               DevState *st, int *gbest_nodes,
+                                               int *gbest_lens, EpochRec *log) {
   if (*(volatile int *)&st->skip) return;
   __shared__ double s_cost[32];
   __shared__ int s_ant[32];
@@ -995,31 +1011,132 @@ __global__ void __launch_bounds__(1024) k_best_t(InstanceView iv, AntBuffers ab,
     for (int t = threadIdx.x; t < total; t += blockDim.x) gbest_nodes[t] = src[t];
     for (int v = threadIdx.x; v < iv.K; v += blockDim.x) gbest_lens[v] = sl[v];
   }
-  if (DEPOSIT) {
-    if (s_best == INT_MAX) return;  // no feasible ant: no evaporation, no deposit
-    __syncthreads();                // the global-best copy is complete
-    const bool sel = *(volatile int *)&st->tau_sel != 0;
-    PheromoneView pd = pv;
-    pd.tau = sel ? pv.tau : tau_alt;  // the evaporated copy
-    const size_t stride_n = (size_t)iv.n + 1;
-    extern __shared__ int s_off[];
-    int *offs = (iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
-    const float dep_i = *(volatile float *)&st->dep_iter;
-    const float dep_g = *(volatile float *)&st->dep_global;
-    deposit_solution(pd, stride_n, CompactNodes{ab.routes + (size_t)s_best * iv.route_stride},
-                     ab.lens + (size_t)s_best * iv.K, iv.K, dep_i, offs);
+}
+
+// The pipelined epoch's iteration best, bookkeeping and both deposits over a
+// cluster of kBestCluster blocks, so that the deposits' scattered pheromone
+// reads and writes are issued from as many SMs.  Every block finds the same
+// iteration best and, from the same state snapshot, the same deposit
+// amounts; block 0 alone keeps the bookkeeping (state, log, global-best
+// copy).  The cluster barrier puts the iteration-best deposit before the
+// global-best one.
+constexpr int kBestCluster = 8;
+constexpr int kBestThreads = 256;
+
+__global__ void __cluster_dims__(kBestCluster, 1, 1) __launch_bounds__(kBestThreads)
+    k_best_cluster(InstanceView iv, AntBuffers ab, DevState *st, int *gbest_nodes,
+                   int *gbest_lens, EpochRec *log, PheromoneView pv, uint8_t *tau_alt) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  __shared__ DevState s_st;
+  __shared__ double s_cost[kBestThreads / 32];
+  __shared__ int s_ant[kBestThreads / 32];
+  __shared__ unsigned long long s_steps[kBestThreads / 32];
+  __shared__ int s_improved, s_best;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  state_load(&s_st, st);
+  double bc = DBL_MAX;
+  int ba = INT_MAX;
+  unsigned long long steps = 0;
+  for (int i = threadIdx.x; i < iv.m; i += blockDim.x) {
+    steps += (unsigned long long)ab.steps[i];
+    if (ab.feasible[i]) {
+      const double c = ab.cost[i];
+      if (ba == INT_MAX || c < bc) {  // ascending i: first minimum kept
+        bc = c;
+        ba = i;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double oc = __shfl_down_sync(kFull, bc, o);
+    const int oa = __shfl_down_sync(kFull, ba, o);
+    steps += __shfl_down_sync(kFull, steps, o);
+    if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
+      bc = oc;
+      ba = oa;
+    }
+  }
+  if (lane == 0) {
+    s_cost[warp] = bc;
+    s_ant[warp] = ba;
+    s_steps[warp] = steps;
+  }
+  __syncthreads();
+  if (s_st.skip) return;  // the same in every block: nothing is written
+  if (warp == 0) {
+    constexpr int nw = kBestThreads / 32;
+    bc = (lane < nw) ? s_cost[lane] : DBL_MAX;
+    ba = (lane < nw) ? s_ant[lane] : INT_MAX;
+    steps = (lane < nw) ? s_steps[lane] : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double oc = __shfl_down_sync(kFull, bc, o);
+      const int oa = __shfl_down_sync(kFull, ba, o);
+      steps += __shfl_down_sync(kFull, steps, o);
+      if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
+        bc = oc;
+        ba = oa;
+      }
+    }
+    if (lane == 0) {
+      // Each block updates its own copy; only block 0's copy and log entry
+      // are kept (the others differ at most in the elapsed-time fields).
+      s_improved = epoch_bookkeeping(&s_st, ba != INT_MAX, bc, ba, steps,
+                                     rank == 0 ? log : nullptr);
+      s_best = ba;
+    }
+  }
+  __syncthreads();
+  const int R = iv.route_stride;
+  if (rank == 0 && s_improved) {
+    // New global best: keep a copy (aco_cuda.cu:367-380).
+    const int *src = ab.routes + (size_t)s_best * R;
+    const int *sl = ab.lens + (size_t)s_best * iv.K;
+    int total = 0;
+    for (int v = 0; v < iv.K; ++v) total += sl[v];
+    for (int t = threadIdx.x; t < total; t += blockDim.x) gbest_nodes[t] = src[t];
+    for (int v = threadIdx.x; v < iv.K; v += blockDim.x) gbest_lens[v] = sl[v];
+  }
+  if (s_best == INT_MAX) {
+    // No feasible ant: no evaporation, no deposit; every block has read the
+    // state before block 0 writes it back.
+    cluster.sync();
+    if (rank == 0) state_store(st, &s_st);
+    return;
+  }
+  const bool sel = s_st.tau_sel != 0;
+  PheromoneView pd = pv;
+  pd.tau = sel ? pv.tau : tau_alt;  // the evaporated copy
+  const size_t stride_n = (size_t)iv.n + 1;
+  extern __shared__ int s_off[];
+  int *offs = (iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
+  const int gt = rank * kBestThreads + (int)threadIdx.x, gn = kBestCluster * kBestThreads;
+  const int *it_nodes = ab.routes + (size_t)s_best * R;
+  const int *it_lens = ab.lens + (size_t)s_best * iv.K;
+  deposit_solution(pd, stride_n, CompactNodes{it_nodes}, it_lens, iv.K, s_st.dep_iter, offs,
+                   gt, gn);
+  // The iteration-best deposit's stores before the global-best deposit's
+  // loads, in every block (release / acquire at cluster scope).
+  cluster.sync();
+  // The global best is this epoch's iteration best when it improved (the
+  // copy block 0 makes holds the same routes).
+  deposit_solution(pd, stride_n, CompactNodes{s_improved ? it_nodes : gbest_nodes},
+                   s_improved ? it_lens : gbest_lens, iv.K, s_st.dep_global, offs, gt, gn);
+  if (rank == 0) {
     __syncthreads();
-    deposit_solution(pd, stride_n, CompactNodes{gbest_nodes}, gbest_lens, iv.K, dep_g, offs);
+    if (threadIdx.x == 0) s_st.tau_sel = sel ? 0 : 1;
     __syncthreads();
-    if (threadIdx.x == 0) st->tau_sel = sel ? 0 : 1;
+    state_store(st, &s_st);
   }
 }
 
 cudaError_t launch_best(const InstanceView &iv, const AntBuffers &ab,
                         DevState *st, int *gbest_nodes, int *gbest_lens,
                         EpochRec *log, cudaStream_t s) {
-  k_best_t<false><<<1, 1024, 0, s>>>(iv, ab, st, gbest_nodes, gbest_lens, log, PheromoneView{},
-                                     nullptr);
+  k_best<<<1, 1024, 0, s>>>(iv, ab, st, gbest_nodes, gbest_lens, log);
   return cudaGetLastError();
 }
 
@@ -1028,7 +1145,8 @@ cudaError_t launch_best_deposit(const InstanceView &iv, const AntBuffers &ab,
                                 int *gbest_nodes, int *gbest_lens, EpochRec *log,
                                 cudaStream_t s) {
   const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
-  k_best_t<true><<<1, 1024, smem, s>>>(iv, ab, st, gbest_nodes, gbest_lens, log, pv, tau_alt);
+  k_best_cluster<<<kBestCluster, kBestThreads, smem, s>>>(iv, ab, st, gbest_nodes, gbest_lens,
+                                                          log, pv, tau_alt);
   return cudaGetLastError();
 }
 
@@ -1343,7 +1461,7 @@ __global__ void __launch_bounds__(256) k_shard_select(InstanceView iv, DevState 
     if (s_improved) gbest_nodes[t] = pk[6 + iv.K + t];
   }
   // Deposits into the buffer the side stream evaporated into during the
-  // construction, then the switch (as k_best_t<true>).
+  // construction, then the switch (as k_best_cluster).
   __syncthreads();
   const bool sel = *(volatile int *)&st->tau_sel != 0;
   PheromoneView pd = pv;

@@ -1418,14 +1418,21 @@ __global__ void __launch_bounds__(1024) k_shard_pack(InstanceView iv, AntBuffers
 // same bookkeeping as k_best; its route goes to iter_nodes/iter_lens and,
 // on improvement, to the global best; then both deposits into the
 // evaporated pheromone buffer and the buffer switch.
-__global__ void __launch_bounds__(256) k_shard_select(InstanceView iv, DevState *st,
-                                                      const int *recv, int world,
-                                                      int *iter_nodes, int *iter_lens,
-                                                      int *gbest_nodes, int *gbest_lens,
-                                                      EpochRec *log,
-                                                      PheromoneView pv, uint8_t *tau_alt) {
-  if (*(volatile int *)&st->skip) return;
+__global__ void __cluster_dims__(kBestCluster, 1, 1) __launch_bounds__(kBestThreads)
+    k_shard_select(InstanceView iv, DevState *st, const int *recv, int world, int *iter_nodes,
+                   int *iter_lens, int *gbest_nodes, int *gbest_lens, EpochRec *log,
+                   PheromoneView pv, uint8_t *tau_alt) {
+  // A cluster like k_best_cluster: every block selects the same winner and
+  // deposit amounts from the same packets and state snapshot, block 0 keeps
+  // the bookkeeping and the copies, the deposits' arcs are shared out over
+  // the cluster with a barrier between the two deposits.
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  __shared__ DevState s_st;
   __shared__ int s_src, s_improved;
+  state_load(&s_st, st);
+  if (s_st.skip) return;  // the same in every block: nothing is written
   const int P = shard_packet_ints(iv.n, iv.K);
   if (threadIdx.x == 0) {
     double bc = DBL_MAX;
@@ -1444,38 +1451,52 @@ __global__ void __launch_bounds__(256) k_shard_select(InstanceView iv, DevState 
         src = r;
       }
     }
-    s_improved = epoch_bookkeeping(st, src >= 0, bc, ba, steps, log);
+    s_improved = epoch_bookkeeping(&s_st, src >= 0, bc, ba, steps, rank == 0 ? log : nullptr);
     s_src = src;
   }
   __syncthreads();
-  if (s_src < 0) return;
-  const int *pk = recv + (size_t)s_src * P;
-  int total = 0;
-  for (int v = 0; v < iv.K; ++v) total += pk[6 + v];
-  for (int v = threadIdx.x; v < iv.K; v += blockDim.x) {
-    iter_lens[v] = pk[6 + v];
-    if (s_improved) gbest_lens[v] = pk[6 + v];
+  if (s_src < 0) {
+    // No feasible ant anywhere: no evaporation, no deposit; every block has
+    // read the state before block 0 writes it back.
+    cluster.sync();
+    if (rank == 0) state_store(st, &s_st);
+    return;
   }
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    iter_nodes[t] = pk[6 + iv.K + t];
-    if (s_improved) gbest_nodes[t] = pk[6 + iv.K + t];
+  const int *pk = recv + (size_t)s_src * P;
+  const int *w_lens = pk + 6;
+  const int *w_nodes = pk + 6 + iv.K;
+  if (rank == 0) {
+    int total = 0;
+    for (int v = 0; v < iv.K; ++v) total += w_lens[v];
+    for (int v = threadIdx.x; v < iv.K; v += blockDim.x) {
+      iter_lens[v] = w_lens[v];
+      if (s_improved) gbest_lens[v] = w_lens[v];
+    }
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+      iter_nodes[t] = w_nodes[t];
+      if (s_improved) gbest_nodes[t] = w_nodes[t];
+    }
   }
   // Deposits into the buffer the side stream evaporated into during the
-  // construction, then the switch (as k_best_cluster).
-  __syncthreads();
-  const bool sel = *(volatile int *)&st->tau_sel != 0;
+  // construction, read straight from the winning packet.
+  const bool sel = s_st.tau_sel != 0;
   PheromoneView pd = pv;
   pd.tau = sel ? pv.tau : tau_alt;
   const size_t stride_n = (size_t)iv.n + 1;
   extern __shared__ int s_off[];
   int *offs = (iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
-  const float dep_i = *(volatile float *)&st->dep_iter;
-  const float dep_g = *(volatile float *)&st->dep_global;
-  deposit_solution(pd, stride_n, CompactNodes{iter_nodes}, iter_lens, iv.K, dep_i, offs);
-  __syncthreads();
-  deposit_solution(pd, stride_n, CompactNodes{gbest_nodes}, gbest_lens, iv.K, dep_g, offs);
-  __syncthreads();
-  if (threadIdx.x == 0) st->tau_sel = sel ? 0 : 1;
+  const int gt = rank * kBestThreads + (int)threadIdx.x, gn = kBestCluster * kBestThreads;
+  deposit_solution(pd, stride_n, CompactNodes{w_nodes}, w_lens, iv.K, s_st.dep_iter, offs, gt,
+                   gn);
+  cluster.sync();
+  deposit_solution(pd, stride_n, CompactNodes{s_improved ? w_nodes : gbest_nodes},
+                   s_improved ? w_lens : gbest_lens, iv.K, s_st.dep_global, offs, gt, gn);
+  if (rank == 0) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_st.tau_sel = sel ? 0 : 1;
+    __syncthreads();
+    state_store(st, &s_st);
+  }
 }
 
 int shard_packet_size(int n, int K) { return shard_packet_ints(n, K); }
@@ -1491,8 +1512,9 @@ cudaError_t launch_shard_select(const InstanceView &iv, DevState *st, const int 
                                 int *gbest_nodes, int *gbest_lens, EpochRec *log,
                                 const PheromoneView &pv, uint8_t *tau_alt, cudaStream_t s) {
   const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
-  k_shard_select<<<1, 256, smem, s>>>(iv, st, recv, world, iter_nodes, iter_lens, gbest_nodes,
-                                      gbest_lens, log, pv, tau_alt);
+  k_shard_select<<<kBestCluster, kBestThreads, smem, s>>>(iv, st, recv, world, iter_nodes,
+                                                          iter_lens, gbest_nodes, gbest_lens,
+                                                          log, pv, tau_alt);
   return cudaGetLastError();
 }
 

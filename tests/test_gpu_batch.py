@@ -101,3 +101,21 @@ def test_setup_reuse_and_get_all(reference_runs):
                 want = ref[i][:3] if batch is not large else want_large[i][:3]
                 assert cost == want[2], (i, cost, want[2])
                 assert np.array_equal(nodes, want[0]) and np.array_equal(lens, want[1])
+
+
+def test_batch_with_an_unservable_instance():
+    """An instance no ant can serve ends with no solution (infinite cost, no
+    routes, pheromone untouched by the deposits) without disturbing the
+    others, which equal the single-instance solver."""
+    from tests.test_gpu_sharding import _unservable
+    insts = [mixed_instances()[0], _unservable(), mixed_instances()[2]]
+    want = [plain(insts[i], 40 + i, 16, 8, 10) for i in (0, 2)]
+    with _native.Batch(0) as b:
+        b.setup(insts, ants=16, cand_k=8, seed=40, epochs=10)
+        b.solve()
+        got = b.best_all()
+        costs, epochs, steps = b.costs()
+    assert got[1][2] == float("inf") and got[1][0].size == 0
+    assert np.all(epochs == 10)
+    for g, (rn, rl, rc, re) in zip((got[0], got[2]), want):
+        assert g[2] == rc and np.array_equal(g[0], rn) and np.array_equal(g[1], rl)

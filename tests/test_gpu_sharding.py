@@ -114,6 +114,50 @@ def test_stop_rules_agree_across_shards(native):
     whole.close()
 
 
+def _unservable():
+    # customer 60 needs 61 of a capacity of 60: no ant is ever feasible
+    rs = np.random.RandomState(5)
+    pts = [(500, 500)] + [tuple(rs.randint(0, 1001, 2)) for _ in range(60)]
+    x = np.array([p[0] for p in pts], np.float32)
+    y = np.array([p[1] for p in pts], np.float32)
+    d = np.array([0] + [5] * 59 + [61], np.int32)
+    return I.Instance("big", x, y, d, 6, 60)
+
+
+def test_shards_without_a_feasible_ant(native):
+    """No rank has a feasible ant: the select kernel leaves the pheromone and
+    the best alone and keeps the same bookkeeping as one colony."""
+    import torch
+    inst = _unservable()
+    s = torch.cuda.Stream()
+    whole = _setup(native, inst, 8, 16, 0, s)
+    parts = [_setup(native, inst, 8, 8, r * 8, s) for r in range(2)]
+    t0 = whole.tau()
+    P = parts[0].shard_packet_ints()
+    send = [torch.zeros(P, dtype=torch.int32, device="cuda") for _ in parts]
+    recv = torch.zeros(2 * P, dtype=torch.int32, device="cuda")
+    for e in range(6):
+        for c, b in zip(parts, send):
+            c.shard_construct(b.data_ptr())
+        with torch.cuda.stream(s):
+            recv[:P].copy_(send[0])
+            recv[P:].copy_(send[1])
+        for c in parts:
+            c.shard_update(recv.data_ptr(), 2)
+        whole.enqueue_epochs(1)
+    s.synchronize()
+    sw = whole.state()
+    assert sw.epochs == 6 and not sw.found and sw.iter_since_best == 6
+    for c in parts + [whole]:
+        st = c.state()
+        assert (st.epochs, st.found, st.iter_since_best, st.total_steps, st.error) == \
+            (sw.epochs, sw.found, sw.iter_since_best, sw.total_steps, 0)
+        assert np.array_equal(c.tau(), t0)
+        nodes, lens, cost = c.best()
+        assert cost == float("inf") and nodes.size == 0
+        c.close()
+
+
 def test_sharded_colony_over_nccl_world_one(native):
     """ShardedColony through a real NCCL process group (one rank) follows the
     plain context epoch for epoch."""

@@ -546,7 +546,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
           continue;
         }
       }
-      const int src = __ffs(msk) - 1;  // -1 (lane 31) only when denom == 0
+      const int src = __ffs(msk) - 1;  // msk != 0 here: denom > 0
       int next = __shfl_sync(kFull, c, src);
       int dn = UNIT ? 1 : __shfl_sync(kFull, dc, src);
       bool drawn = false;  // draws of this step already accounted

@@ -596,9 +596,9 @@ def run_batched(args, rank, world, local, torch, dist, _native):
             b2.solve()
             res = b2.best_all()
             dt = time.perf_counter() - t0
+            assert len(res) == len(insts)
             if i > 0:
                 e2e_vals.append(len(insts) / dt)
-        assert len(res) == len(insts)
     e2e = statistics.median(e2e_vals) if e2e_vals else None
     if world > 1:
         te = torch.tensor([e2e or 0.0], dtype=torch.float64, device="cuda")

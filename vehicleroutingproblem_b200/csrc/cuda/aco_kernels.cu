@@ -943,40 +943,46 @@ __device__ __forceinline__ uint32_t evap4(uint32_t x, uint32_t floor4,
   return __vsub4(__vmaxu4(x, floor4), delta4);
 }
 
-// Iteration best, bookkeeping and the global-best copy in one block, for the
-// epochs whose pheromone update is a separate k_evap_deposit launch.
-__global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
-                                               DevState *st, int *gbest_nodes,
-                                               int *gbest_lens, EpochRec *log) {
-  if (*(volatile int *)&st->skip) return;
-  __shared__ double s_cost[32];
-  __shared__ int s_ant[32];
-  __shared__ unsigned long long s_steps[32];
-  __shared__ int s_improved, s_best;
+// Folds (oc, oa) into the running best (bc, ba): least cost, then lowest
+// ant (the first minimum of select_iter_best_host, src/cuda/aco_cuda.cu:96-126).
+__device__ __forceinline__ void best_fold(double &bc, int &ba, double oc, int oa) {
+  if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
+    bc = oc;
+    ba = oa;
+  }
+}
+
+__device__ __forceinline__ void warp_best(double &bc, int &ba, unsigned long long &steps) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double oc = __shfl_down_sync(kFull, bc, o);
+    const int oa = __shfl_down_sync(kFull, ba, o);
+    steps += __shfl_down_sync(kFull, steps, o);
+    best_fold(bc, ba, oc, oa);
+  }
+}
+
+// Iteration best of the m ants (INT_MAX: none feasible) and their
+// ant-steps, over one block; every thread calls it, lane 0 of warp 0 holds
+// the result.  The s_* scratch holds one entry per warp.
+__device__ __forceinline__ void block_iter_best(const AntBuffers &ab, int m, double *s_cost,
+                                                int *s_ant, unsigned long long *s_steps,
+                                                double &bc, int &ba, unsigned long long &steps) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double bc = DBL_MAX;
-  int ba = INT_MAX;
-  unsigned long long steps = 0;
-  for (int i = threadIdx.x; i < iv.m; i += blockDim.x) {
+  bc = DBL_MAX;
+  ba = INT_MAX;
+  steps = 0;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
     steps += (unsigned long long)ab.steps[i];
     if (ab.feasible[i]) {
-      double c = ab.cost[i];
+      const double c = ab.cost[i];
       if (ba == INT_MAX || c < bc) {  // ascending i: first minimum kept
         bc = c;
         ba = i;
       }
     }
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    double oc = __shfl_down_sync(kFull, bc, o);
-    int oa = __shfl_down_sync(kFull, ba, o);
-    steps += __shfl_down_sync(kFull, steps, o);
-    if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
-      bc = oc;
-      ba = oa;
-    }
-  }
+  warp_best(bc, ba, steps);
   if (lane == 0) {
     s_cost[warp] = bc;
     s_ant[warp] = ba;
@@ -988,21 +994,27 @@ __global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
     bc = (lane < nw) ? s_cost[lane] : DBL_MAX;
     ba = (lane < nw) ? s_ant[lane] : INT_MAX;
     steps = (lane < nw) ? s_steps[lane] : 0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      double oc = __shfl_down_sync(kFull, bc, o);
-      int oa = __shfl_down_sync(kFull, ba, o);
-      steps += __shfl_down_sync(kFull, steps, o);
-      if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
-        bc = oc;
-        ba = oa;
-      }
-    }
-    if (lane == 0) {
-      const int improved = epoch_bookkeeping(st, ba != INT_MAX, bc, ba, steps, log);
-      s_improved = improved;
-      s_best = ba;
-    }
+    warp_best(bc, ba, steps);
+  }
+}
+
+// Iteration best, bookkeeping and the global-best copy in one block, for the
+// epochs whose pheromone update is a separate k_evap_deposit launch.
+__global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
+                                               DevState *st, int *gbest_nodes,
+                                               int *gbest_lens, EpochRec *log) {
+  if (*(volatile int *)&st->skip) return;
+  __shared__ double s_cost[32];
+  __shared__ int s_ant[32];
+  __shared__ unsigned long long s_steps[32];
+  __shared__ int s_improved, s_best;
+  double bc;
+  int ba;
+  unsigned long long steps;
+  block_iter_best(ab, iv.m, s_cost, s_ant, s_steps, bc, ba, steps);
+  if (threadIdx.x == 0) {
+    s_improved = epoch_bookkeeping(st, ba != INT_MAX, bc, ba, steps, log);
+    s_best = ba;
   }
   __syncthreads();
   if (s_improved) {
@@ -1027,6 +1039,36 @@ __global__ void __launch_bounds__(1024) k_best(InstanceView iv, AntBuffers ab,
 constexpr int kBestCluster = 8;
 constexpr int kBestThreads = 256;
 
+// The epoch's two deposits over the cluster, into the buffer evaporated
+// beside the construction: the iteration best, a cluster barrier (its stores
+// before the next deposit's loads, release / acquire at cluster scope), the
+// global best; then block 0 switches the buffer and writes the state back.
+__device__ __forceinline__ void cluster_deposits(cooperative_groups::cluster_group &cluster,
+                                                 int rank, const InstanceView &iv,
+                                                 const PheromoneView &pv, uint8_t *tau_alt,
+                                                 DevState *s_st, DevState *st,
+                                                 const int *it_nodes, const int *it_lens,
+                                                 const int *gb_nodes, const int *gb_lens) {
+  const bool sel = s_st->tau_sel != 0;
+  PheromoneView pd = pv;
+  pd.tau = sel ? pv.tau : tau_alt;  // the evaporated copy
+  const size_t stride_n = (size_t)iv.n + 1;
+  extern __shared__ int s_off[];
+  int *offs = (iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
+  const int gt = rank * kBestThreads + (int)threadIdx.x, gn = kBestCluster * kBestThreads;
+  deposit_solution(pd, stride_n, CompactNodes{it_nodes}, it_lens, iv.K, s_st->dep_iter, offs, gt,
+                   gn);
+  cluster.sync();
+  deposit_solution(pd, stride_n, CompactNodes{gb_nodes}, gb_lens, iv.K, s_st->dep_global, offs,
+                   gt, gn);
+  if (rank == 0) {
+    __syncthreads();
+    if (threadIdx.x == 0) s_st->tau_sel = sel ? 0 : 1;
+    __syncthreads();
+    state_store(st, s_st);
+  }
+}
+
 __global__ void __cluster_dims__(kBestCluster, 1, 1) __launch_bounds__(kBestThreads)
     k_best_cluster(InstanceView iv, AntBuffers ab, DevState *st, int *gbest_nodes,
                    int *gbest_lens, EpochRec *log, PheromoneView pv, uint8_t *tau_alt) {
@@ -1038,60 +1080,17 @@ __global__ void __cluster_dims__(kBestCluster, 1, 1) __launch_bounds__(kBestThre
   __shared__ int s_ant[kBestThreads / 32];
   __shared__ unsigned long long s_steps[kBestThreads / 32];
   __shared__ int s_improved, s_best;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   state_load(&s_st, st);
-  double bc = DBL_MAX;
-  int ba = INT_MAX;
-  unsigned long long steps = 0;
-  for (int i = threadIdx.x; i < iv.m; i += blockDim.x) {
-    steps += (unsigned long long)ab.steps[i];
-    if (ab.feasible[i]) {
-      const double c = ab.cost[i];
-      if (ba == INT_MAX || c < bc) {  // ascending i: first minimum kept
-        bc = c;
-        ba = i;
-      }
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double oc = __shfl_down_sync(kFull, bc, o);
-    const int oa = __shfl_down_sync(kFull, ba, o);
-    steps += __shfl_down_sync(kFull, steps, o);
-    if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
-      bc = oc;
-      ba = oa;
-    }
-  }
-  if (lane == 0) {
-    s_cost[warp] = bc;
-    s_ant[warp] = ba;
-    s_steps[warp] = steps;
-  }
-  __syncthreads();
+  double bc;
+  int ba;
+  unsigned long long steps;
+  block_iter_best(ab, iv.m, s_cost, s_ant, s_steps, bc, ba, steps);
   if (s_st.skip) return;  // the same in every block: nothing is written
-  if (warp == 0) {
-    constexpr int nw = kBestThreads / 32;
-    bc = (lane < nw) ? s_cost[lane] : DBL_MAX;
-    ba = (lane < nw) ? s_ant[lane] : INT_MAX;
-    steps = (lane < nw) ? s_steps[lane] : 0ull;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double oc = __shfl_down_sync(kFull, bc, o);
-      const int oa = __shfl_down_sync(kFull, ba, o);
-      steps += __shfl_down_sync(kFull, steps, o);
-      if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
-        bc = oc;
-        ba = oa;
-      }
-    }
-    if (lane == 0) {
-      // Each block updates its own copy; only block 0's copy and log entry
-      // are kept (the others differ at most in the elapsed-time fields).
-      s_improved = epoch_bookkeeping(&s_st, ba != INT_MAX, bc, ba, steps,
-                                     rank == 0 ? log : nullptr);
-      s_best = ba;
-    }
+  if (threadIdx.x == 0) {
+    // Each block updates its own copy; only block 0's copy and log entry are
+    // kept (the others differ at most in the elapsed-time fields).
+    s_improved = epoch_bookkeeping(&s_st, ba != INT_MAX, bc, ba, steps, rank == 0 ? log : nullptr);
+    s_best = ba;
   }
   __syncthreads();
   const int R = iv.route_stride;
@@ -1111,30 +1110,12 @@ __global__ void __cluster_dims__(kBestCluster, 1, 1) __launch_bounds__(kBestThre
     if (rank == 0) state_store(st, &s_st);
     return;
   }
-  const bool sel = s_st.tau_sel != 0;
-  PheromoneView pd = pv;
-  pd.tau = sel ? pv.tau : tau_alt;  // the evaporated copy
-  const size_t stride_n = (size_t)iv.n + 1;
-  extern __shared__ int s_off[];
-  int *offs = (iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
-  const int gt = rank * kBestThreads + (int)threadIdx.x, gn = kBestCluster * kBestThreads;
   const int *it_nodes = ab.routes + (size_t)s_best * R;
   const int *it_lens = ab.lens + (size_t)s_best * iv.K;
-  deposit_solution(pd, stride_n, CompactNodes{it_nodes}, it_lens, iv.K, s_st.dep_iter, offs,
-                   gt, gn);
-  // The iteration-best deposit's stores before the global-best deposit's
-  // loads, in every block (release / acquire at cluster scope).
-  cluster.sync();
   // The global best is this epoch's iteration best when it improved (the
   // copy block 0 makes holds the same routes).
-  deposit_solution(pd, stride_n, CompactNodes{s_improved ? it_nodes : gbest_nodes},
-                   s_improved ? it_lens : gbest_lens, iv.K, s_st.dep_global, offs, gt, gn);
-  if (rank == 0) {
-    __syncthreads();
-    if (threadIdx.x == 0) s_st.tau_sel = sel ? 0 : 1;
-    __syncthreads();
-    state_store(st, &s_st);
-  }
+  cluster_deposits(cluster, rank, iv, pv, tau_alt, &s_st, st, it_nodes, it_lens,
+                   s_improved ? it_nodes : gbest_nodes, s_improved ? it_lens : gbest_lens);
 }
 
 cudaError_t launch_best(const InstanceView &iv, const AntBuffers &ab,
@@ -1353,50 +1334,12 @@ __global__ void __launch_bounds__(1024) k_shard_pack(InstanceView iv, AntBuffers
   __shared__ int s_ant[32];
   __shared__ unsigned long long s_steps[32];
   __shared__ int s_best;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const bool skip = *(volatile int *)&st->skip;
-  double bc = DBL_MAX;
-  int ba = INT_MAX;
-  unsigned long long steps = 0;
-  for (int i = threadIdx.x; i < iv.m && !skip; i += blockDim.x) {
-    steps += (unsigned long long)ab.steps[i];
-    if (ab.feasible[i]) {
-      const double c = ab.cost[i];
-      if (ba == INT_MAX || c < bc) {
-        bc = c;
-        ba = i;
-      }
-    }
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double oc = __shfl_down_sync(kFull, bc, o);
-    const int oa = __shfl_down_sync(kFull, ba, o);
-    steps += __shfl_down_sync(kFull, steps, o);
-    if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
-      bc = oc;
-      ba = oa;
-    }
-  }
-  if (lane == 0) {
-    s_cost[warp] = bc;
-    s_ant[warp] = ba;
-    s_steps[warp] = steps;
-  }
-  __syncthreads();
+  double bc;
+  int ba;
+  unsigned long long steps;
+  block_iter_best(ab, skip ? 0 : iv.m, s_cost, s_ant, s_steps, bc, ba, steps);
   if (threadIdx.x == 0) {
-    bc = DBL_MAX;
-    ba = INT_MAX;
-    steps = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-      steps += s_steps[w];
-      const double oc = s_cost[w];
-      const int oa = s_ant[w];
-      if (oa != INT_MAX && (ba == INT_MAX || oc < bc || (oc == bc && oa < ba))) {
-        bc = oc;
-        ba = oa;
-      }
-    }
     const unsigned long long cb = (unsigned long long)__double_as_longlong(bc);
     send[0] = (int)(cb & 0xffffffffu);
     send[1] = (int)(cb >> 32);
@@ -1481,26 +1424,9 @@ __global__ void __cluster_dims__(kBestCluster, 1, 1) __launch_bounds__(kBestThre
       if (s_improved) gbest_nodes[t] = w_nodes[t];
     }
   }
-  // Deposits into the buffer the side stream evaporated into during the
-  // construction, read straight from the winning packet.
-  const bool sel = s_st.tau_sel != 0;
-  PheromoneView pd = pv;
-  pd.tau = sel ? pv.tau : tau_alt;
-  const size_t stride_n = (size_t)iv.n + 1;
-  extern __shared__ int s_off[];
-  int *offs = (iv.K <= kDepositSmemRoutes) ? s_off : nullptr;
-  const int gt = rank * kBestThreads + (int)threadIdx.x, gn = kBestCluster * kBestThreads;
-  deposit_solution(pd, stride_n, CompactNodes{w_nodes}, w_lens, iv.K, s_st.dep_iter, offs, gt,
-                   gn);
-  cluster.sync();
-  deposit_solution(pd, stride_n, CompactNodes{s_improved ? w_nodes : gbest_nodes},
-                   s_improved ? w_lens : gbest_lens, iv.K, s_st.dep_global, offs, gt, gn);
-  if (rank == 0) {
-    __syncthreads();
-    if (threadIdx.x == 0) s_st.tau_sel = sel ? 0 : 1;
-    __syncthreads();
-    state_store(st, &s_st);
-  }
+  // The deposits read the winner straight from its packet.
+  cluster_deposits(cluster, rank, iv, pv, tau_alt, &s_st, st, w_nodes, w_lens,
+                   s_improved ? w_nodes : gbest_nodes, s_improved ? w_lens : gbest_lens);
 }
 
 int shard_packet_size(int n, int K) { return shard_packet_ints(n, K); }

@@ -258,8 +258,11 @@ struct Tables {
   }
 };
 
-// Visited set of one ant.  V = 1 or 2: lane L holds bitmap words L (and
-// L + 32) in registers (n < 2048); V = 0: the bitmap is in shared memory.
+// Visited set of one ant.  V = 1 or 2 (n < 2048): registers, transposed so
+// that lane L holds nodes L, L + 32, L + 64, ... (and from 1024 on in a
+// second word): the nodes of any instance spread evenly over the lanes,
+// which keeps the nearest-customer scan short on small instances.  V = 0:
+// the bitmap is in shared memory, word wi holding nodes 32 wi .. 32 wi + 31.
 // The depot and the bits past node n start set.  test/set are collective.
 __device__ __forceinline__ uint32_t vis_init_word(int wi, int n) {
   uint32_t word = 0u;
@@ -281,34 +284,42 @@ struct Visited {
     vw = vw_;
     s = smem_words;
     w0 = w1 = 0xffffffffu;
-    if (V >= 1) w0 = vis_init_word(lane, n);
-    if (V == 2) w1 = vis_init_word(lane + 32, n);
+    // Registers hold the bitmap transposed: bit b of lane L's w0 is node
+    // L + 32 b, of its w1 node 1024 + L + 32 b.
+    if (V >= 1) w0 = lane_word(lane, n) | (lane == 0 ? 1u : 0u);
+    if (V == 2) w1 = lane_word(1024 + lane, n);
     if (V == 0) {
       for (int wi = lane; wi < vw; wi += 32) s[wi] = vis_init_word(wi, n);
       __syncwarp();
     }
   }
-  // Bitmap word holding node c (the shuffle source lane is taken modulo 32).
-  __device__ __forceinline__ uint32_t word_of(int c) const {
-    if (V == 0) return s[c >> 5];
-    uint32_t word = __shfl_sync(kFull, w0, c >> 5);
-    if (V == 2) {
-      const uint32_t hi = __shfl_sync(kFull, w1, c >> 5);
-      word = (c >> 10) ? hi : word;
-    }
-    return word;
+  // Nodes first + 32 b (b = 0..31) that are beyond n: their bits start set.
+  __device__ __forceinline__ static uint32_t lane_word(int first, int n) {
+    const int cnt = n >= first ? (n - first) / 32 + 1 : 0;  // nodes <= n
+    return cnt >= 32 ? 0u : (0xffffffffu << cnt);
   }
   __device__ __forceinline__ bool test(int c) const {
-    const uint32_t word = word_of(c);
-    return (__funnelshift_r(word, word, c) & 1u) != 0u;  // bit c mod 32
+    if (V == 0) {
+      const uint32_t word = s[c >> 5];
+      return (__funnelshift_r(word, word, c) & 1u) != 0u;  // bit c mod 32
+    }
+    // Lane c mod 32 holds node c (the shuffle takes the source modulo 32),
+    // at bit (c / 32) mod 32.
+    uint32_t word = __shfl_sync(kFull, w0, c);
+    if (V == 2) {
+      const uint32_t hi = __shfl_sync(kFull, w1, c);
+      word = (c >> 10) ? hi : word;
+    }
+    return (__funnelshift_r(word, word, c >> 5) & 1u) != 0u;
   }
   __device__ __forceinline__ void set(int node, int lane) {
-    const uint32_t bit = __funnelshift_l(0u, 1u, node);  // 1 << (node mod 32)
     if (V == 0) {
+      const uint32_t bit = __funnelshift_l(0u, 1u, node);  // 1 << (node mod 32)
       if (lane == 0) s[node >> 5] |= bit;
       __syncwarp();
     } else {
-      const bool mine = lane == (V == 1 ? (node >> 5) : ((node >> 5) & 31));
+      const uint32_t bit = __funnelshift_l(0u, 1u, node >> 5);  // 1 << ((node / 32) mod 32)
+      const bool mine = lane == (node & 31);
       if (V == 2 && (node >> 10)) w1 |= mine ? bit : 0u;
       else w0 |= mine ? bit : 0u;
     }
@@ -324,11 +335,13 @@ __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
                                                  float2 pc, int room,
                                                  bool check_dem, int lane) {
   uint32_t best_h = 0xffffffffu, best_n = 0xffffffffu;
-  auto scan = [&](uint32_t fr, int wi) {
+  // V = 1, 2: bit b of a register word is node first + 32 b (ascending);
+  // V = 0: bit b of word wi is node 32 wi + b.
+  auto scan = [&](uint32_t fr, int first, int step) {
     while (fr) {
       const int b = __ffs(fr) - 1;
       fr &= fr - 1;
-      const int node = (wi << 5) + b;
+      const int node = first + b * step;
       if (!UNIT && check_dem && tb.demand(node) > room) continue;
       const uint32_t h = __float_as_uint(dist2f(pc, tb.coord(node)));
       if (h < best_h) {
@@ -337,10 +350,10 @@ __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
       }
     }
   };
-  if (V >= 1) scan(~vis.w0, lane);
-  if (V == 2) scan(~vis.w1, lane + 32);
+  if (V >= 1) scan(~vis.w0, lane, 32);
+  if (V == 2) scan(~vis.w1, 1024 + lane, 32);
   if (V == 0)
-    for (int wi = lane; wi < vis.vw; wi += 32) scan(~vis.s[wi], wi);
+    for (int wi = lane; wi < vis.vw; wi += 32) scan(~vis.s[wi], wi << 5, 1);
   const uint32_t mh = __reduce_min_sync(kFull, best_h);
   const uint32_t mn = __reduce_min_sync(kFull, best_h == mh ? best_n : 0xffffffffu);
   return (mh == 0xffffffffu) ? 0 : (int)mn;

@@ -123,51 +123,50 @@ struct Seg {
   __device__ __forceinline__ void sync() const { __syncwarp(mask); }
 };
 
-// Visited bitmap of one ant in the segment's registers: lane L holds words
-// L and L + LANES (V = 2).
+// Visited bitmap of one ant in the segment's registers, transposed: bit b
+// of lane L's w0 is node L + LANES b, of its w1 node 32 LANES + L + LANES b
+// (V = 2).  The nodes of any instance spread evenly over the lanes, which
+// keeps the nearest-customer scan short.
 template <int LANES, int V>
 struct SegVisited {
+  static constexpr int kShift = (LANES == 16) ? 4 : 5;  // log2(LANES)
   uint32_t w0, w1;
   __device__ __forceinline__ void init(const Seg<LANES> &sg, int n) {
-    w0 = vis_word(sg.lane, n);
-    w1 = (V == 2) ? vis_word(sg.lane + LANES, n) : 0xffffffffu;
+    w0 = lane_word(sg.lane, n) | (sg.lane == 0 ? 1u : 0u);  // the depot starts visited
+    w1 = (V == 2) ? lane_word(32 * LANES + sg.lane, n) : 0xffffffffu;
   }
-  __device__ __forceinline__ static uint32_t vis_word(int wi, int n) {
-    uint32_t word = 0u;
-    const int lo = wi << 5;
-    if (lo == 0) word |= 1u;
-    const int valid = n + 1 - lo;
-    if (valid < 32) word |= (valid <= 0) ? 0xffffffffu : (0xffffffffu << valid);
-    return word;
+  // Nodes first + LANES b (b = 0..31) beyond n start set.
+  __device__ __forceinline__ static uint32_t lane_word(int first, int n) {
+    const int cnt = n >= first ? (n - first) / LANES + 1 : 0;  // nodes <= n
+    return cnt >= 32 ? 0u : (0xffffffffu << cnt);
   }
   __device__ __forceinline__ bool test(const Seg<LANES> &sg, int c) const {
-    const int wi = c >> 5;
-    uint32_t word = sg.shfl(w0, wi & (LANES - 1));
+    // The shuffle takes the source lane modulo the segment width.
+    uint32_t word = sg.shfl(w0, c);
     if (V == 2) {
-      const uint32_t hi = sg.shfl(w1, wi & (LANES - 1));
-      word = (wi >= LANES) ? hi : word;
+      const uint32_t hi = sg.shfl(w1, c);
+      word = (c >= 32 * LANES) ? hi : word;
     }
-    return __funnelshift_r(word, word, c) & 1u;  // bit c mod 32
+    return __funnelshift_r(word, word, c >> kShift) & 1u;  // bit (c / LANES) mod 32
   }
   __device__ __forceinline__ void set(const Seg<LANES> &sg, int node) {
-    const int wi = node >> 5;
-    const uint32_t bit = __funnelshift_l(0u, 1u, node);  // 1 << (node mod 32)
-    if (sg.lane == (wi & (LANES - 1))) {
-      if (V == 2 && wi >= LANES) w1 |= bit; else w0 |= bit;
+    const uint32_t bit = __funnelshift_l(0u, 1u, node >> kShift);
+    if (sg.lane == (node & (LANES - 1))) {
+      if (V == 2 && node >= 32 * LANES) w1 |= bit; else w0 |= bit;
     }
   }
 };
-
 template <int LANES, int V>
 __device__ __forceinline__ int seg_nearest(const Seg<LANES> &sg, const SegVisited<LANES, V> &vis,
                                            const float2 *coords, const int *dem, bool unit,
                                            float2 pc, int room, bool check_dem) {
   uint32_t best_h = 0xffffffffu, best_n = 0xffffffffu;
-  auto scan = [&](uint32_t fr, int wi) {
+  // Bit b of a word is node first + LANES b: ascending within a lane.
+  auto scan = [&](uint32_t fr, int first) {
     while (fr) {
       const int b = __ffs(fr) - 1;
       fr &= fr - 1;
-      const int node = (wi << 5) + b;
+      const int node = first + b * LANES;
       if (!unit && check_dem && dem[node] > room) continue;
       const uint32_t h = __float_as_uint(dist2f(pc, coords[node]));
       if (h < best_h) {
@@ -177,7 +176,7 @@ __device__ __forceinline__ int seg_nearest(const Seg<LANES> &sg, const SegVisite
     }
   };
   scan(~vis.w0, sg.lane);
-  if (V == 2) scan(~vis.w1, sg.lane + LANES);
+  if (V == 2) scan(~vis.w1, 32 * LANES + sg.lane);
   const uint32_t mh = sg.umin(best_h);
   const uint32_t mn = sg.umin(best_h == mh ? best_n : 0xffffffffu);
   return (mh == 0xffffffffu) ? 0 : (int)mn;

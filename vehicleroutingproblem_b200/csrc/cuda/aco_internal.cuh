@@ -294,6 +294,14 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src,
       : "memory");
 }
 
+// Marks `bytes` of the barrier's expected transaction count as arrived
+// without a copy (used to balance an expectation no copy will meet).
+__device__ __forceinline__ void mbar_complete_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.complete_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(

@@ -713,12 +713,25 @@ __global__ void __launch_bounds__(512, 1) k_construct(ConstructArgs a) {
            pl.vis_words, iv.n, lane);
 
   if (L != kLayoutGlobal) {
-    // Bounded wait for the staged tables; on time-out the block flags the
-    // error, waits (bounded again) for its copies still in flight and exits.
+    // Bounded wait for the staged tables.  The decision is the block's: it
+    // goes on only when every thread saw the tables arrive, so no warp
+    // enters the full-mask collectives of build_ant with lanes or warps
+    // gone.  On time-out the block flags the error, waits (bounded again)
+    // for its copies still in flight and exits.  The injected time-out
+    // expects stage_extra_tx bytes that no copy brings; thread 0 marks them
+    // arrived, so that second wait ends once the real copies have landed.
+    // After a genuine time-out the second wait may run out as well; the
+    // block then exits with the error flag set.
     const uint32_t limit = iv.stage_extra_tx ? (1u << 14) : (1u << 22);
-    if (!mbar_wait_bounded(bar, 0, limit)) {
-      if (lane == 0 && a.st) atomicOr(&a.st->error, kErrStageTimeout);
-      mbar_wait_bounded(bar, 0, limit);
+    const bool ok = __syncthreads_and(mbar_wait_bounded(bar, 0, limit) ? 1 : 0) != 0;
+    if (!ok) {
+      if (threadIdx.x == 0) {
+        if (a.st) atomicOr(&a.st->error, kErrStageTimeout);
+        if (iv.stage_extra_tx) mbar_complete_tx(bar, (uint32_t)iv.stage_extra_tx);
+      }
+      __syncthreads();
+      mbar_wait_bounded(bar, 0, limit << 2);
+      __syncthreads();
       return;
     }
   }

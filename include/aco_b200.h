@@ -117,6 +117,16 @@ ACO_API int aco_b200_synchronize(aco_b200_ctx *ctx);
  * time (ms) into kernel_ms[4]: weights, construct, evaporate, best+deposit. */
 ACO_API int aco_b200_profile_epochs(aco_b200_ctx *ctx, int epochs, float *kernel_ms);
 
+/* Times the pheromone evaporation sweep alone: `launches` launches of the
+ * kernel and grid the epoch graph uses (current buffer into the other one,
+ * which the next epoch overwrites; the current buffer and the solve's
+ * progress are left unchanged, and the run limit is cleared as by
+ * aco_b200_enqueue_epochs), each between two CUDA events on the context
+ * stream.  *ms_per_launch is the mean device time of one launch.  The sweep
+ * moves 2 (n+1)^2 bytes (read + write); the reference's counterpart is
+ * kernel_evaporate_tau (src/cuda/aco_cuda_kernels.cu:145-155). */
+ACO_API int aco_b200_profile_update(aco_b200_ctx *ctx, int launches, float *ms_per_launch);
+
 /* Best solution so far in compact form: K segments [0 c.. 0] back to back
  * (nodes capacity n + 2K), the K segment lengths and the FP64 cost. */
 ACO_API int aco_b200_get_best(aco_b200_ctx *ctx, int *nodes, int *lens, double *cost);

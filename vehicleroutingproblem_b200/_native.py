@@ -32,7 +32,7 @@ EXPORTED = [
     "aco_b200_get_tau", "aco_b200_set_tau", "aco_b200_get_candidates",
     "aco_b200_get_tables", "aco_b200_get_weights", "aco_b200_construct",
     "aco_b200_get_ants", "aco_b200_evaporate_deposit", "aco_b200_build_info",
-    "aco_b200_profile_epochs", "aco_b200_evaporate_deposit_noalloc",
+    "aco_b200_profile_epochs", "aco_b200_profile_update", "aco_b200_evaporate_deposit_noalloc",
     "aco_b200_batch_create", "aco_b200_batch_destroy", "aco_b200_batch_setup",
     "aco_b200_batch_set_stream",
     "aco_b200_batch_set_tuning", "aco_b200_batch_get_tuning", "aco_b200_batch_autotune",
@@ -126,6 +126,7 @@ def load():
         "aco_b200_get_ants": [vp, vp, vp, vp, vp, vp, vp],
         "aco_b200_evaporate_deposit": [vp, i32, f32, vp, vp, f32],
         "aco_b200_profile_epochs": [vp, i32, vp],
+        "aco_b200_profile_update": [vp, i32, vp],
         "aco_b200_batch_create": [vp, i32], "aco_b200_batch_destroy": [vp],
         "aco_b200_batch_set_stream": [vp, vp],
         "aco_b200_batch_setup": [vp, vp], "aco_b200_batch_set_tuning": [vp, vp],
@@ -254,6 +255,14 @@ class Context:
         _check(self._lib.aco_b200_profile_epochs(self._h, epochs, _p(ms)),
                "aco_b200_profile_epochs")
         return ms
+
+    def profile_update(self, launches: int) -> float:
+        """Mean device ms of one launch of the pheromone evaporation sweep
+        (2 (n+1)^2 bytes read + written), timed alone over `launches`."""
+        ms = np.zeros(1, np.float32)
+        _check(self._lib.aco_b200_profile_update(self._h, launches, _p(ms)),
+               "aco_b200_profile_update")
+        return float(ms[0])
 
     def synchronize(self) -> None:
         _check(self._lib.aco_b200_synchronize(self._h), "aco_b200_synchronize")

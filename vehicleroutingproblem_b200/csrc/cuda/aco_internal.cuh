@@ -184,6 +184,7 @@ cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
                                 unsigned int *counter, int grid, uint8_t *tau_alt,
                                 cudaStream_t s);
 cudaError_t launch_set_run_limit(DevState *st, int limit, cudaStream_t s);
+int evap_grid_for(unsigned long long total, int num_sms);
 cudaError_t launch_evaporate_to(const PheromoneView &pv, uint8_t *tau_alt, DevState *st,
                                 int grid, cudaStream_t s);
 cudaError_t launch_best_deposit(const InstanceView &iv, const AntBuffers &ab,

@@ -969,6 +969,63 @@ __device__ __forceinline__ uint32_t evap4(uint32_t x, uint32_t floor4,
   return __vsub4(__vmaxu4(x, floor4), delta4);
 }
 
+// Evaporation sweep of pv.total bytes from src to dst (src == dst: in
+// place), q > q_min + delta ? q - delta : q_min as max(q, q_min + delta) -
+// delta on 16 bytes at a time (kernel_evaporate_tau,
+// src/cuda/aco_cuda_kernels.cu:145-155).  Each thread keeps kEvapUnroll
+// 16-byte loads in flight before its stores (a block covers
+// kEvapUnroll * blockDim.x vectors per trip), and the loads and stores are
+// streaming (evict-first), so a matrix larger than L2 passes through without
+// displacing the construction's tables.  Block 0 also does the tail past the
+// last whole vector.
+constexpr int kEvapUnroll = 4;
+constexpr int kEvapThreads = 512;
+
+__device__ __forceinline__ void evap_sweep(const uint8_t *src, uint8_t *dst,
+                                           unsigned long long total, uint8_t q_min,
+                                           uint8_t delta) {
+  const int fl = (int)q_min + (int)delta;
+  const bool sat_all = fl > 255;
+  const uint32_t floor4 = 0x01010101u * (uint32_t)(sat_all ? 0 : fl);
+  const uint32_t delta4 = 0x01010101u * (uint32_t)delta;
+  const uint32_t qmin4 = 0x01010101u * (uint32_t)q_min;
+  const unsigned long long nvec = total / 16;
+  const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
+  uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+  const unsigned long long tile = (unsigned long long)kEvapUnroll * blockDim.x;
+  const unsigned long long step = tile * gridDim.x;
+  for (unsigned long long base = blockIdx.x * tile + threadIdx.x; base < nvec; base += step) {
+    uint4 v[kEvapUnroll];
+#pragma unroll
+    for (int u = 0; u < kEvapUnroll; ++u) {
+      const unsigned long long i = base + (unsigned long long)u * blockDim.x;
+      if (i < nvec) v[u] = __ldcs(s4 + i);
+    }
+#pragma unroll
+    for (int u = 0; u < kEvapUnroll; ++u) {
+      const unsigned long long i = base + (unsigned long long)u * blockDim.x;
+      if (i < nvec) {
+        uint4 r = v[u];
+        if (sat_all) {
+          r = make_uint4(qmin4, qmin4, qmin4, qmin4);
+        } else {
+          r.x = evap4(r.x, floor4, delta4);
+          r.y = evap4(r.y, floor4, delta4);
+          r.z = evap4(r.z, floor4, delta4);
+          r.w = evap4(r.w, floor4, delta4);
+        }
+        __stcs(d4 + i, r);
+      }
+    }
+  }
+  if (blockIdx.x == 0) {
+    for (unsigned long long i = nvec * 16 + threadIdx.x; i < total; i += blockDim.x) {
+      const uint8_t q = src[i];
+      dst[i] = ((int)q > fl) ? (uint8_t)(q - delta) : q_min;
+    }
+  }
+}
+
 // Folds (oc, oa) into the running best (bc, ba): least cost, then lowest
 // ant (the first minimum of select_iter_best_host, src/cuda/aco_cuda.cu:96-126).
 __device__ __forceinline__ void best_fold(double &bc, int &ba, double oc, int oa) {
@@ -1164,45 +1221,40 @@ cudaError_t launch_best_deposit(const InstanceView &iv, const AntBuffers &ab,
 // Evaporation of the current pheromone buffer into the other one, run beside
 // the construction (which reads only the weights): 16 bytes per thread,
 // max(q, q_min + delta) - delta.
-__global__ void __launch_bounds__(512) k_evaporate_to(PheromoneView pv, uint8_t *tau_alt,
-                                                      DevState *st) {
+__global__ void __launch_bounds__(kEvapThreads) k_evaporate_to(PheromoneView pv,
+                                                               uint8_t *tau_alt, DevState *st) {
   if (*(volatile int *)&st->skip) return;
   const bool sel = *(volatile int *)&st->tau_sel != 0;
   const uint8_t *src = sel ? tau_alt : pv.tau;
   uint8_t *dst = sel ? pv.tau : tau_alt;
-  const int fl = (int)pv.q_min + (int)pv.delta;
-  const bool sat_all = fl > 255;
-  const uint32_t floor4 = 0x01010101u * (uint32_t)(sat_all ? 0 : fl);
-  const uint32_t delta4 = 0x01010101u * (uint32_t)pv.delta;
-  const uint32_t qmin4 = 0x01010101u * (uint32_t)pv.q_min;
-  const unsigned long long nvec = pv.total / 16;
-  const uint4 *s4 = reinterpret_cast<const uint4 *>(src);
-  uint4 *d4 = reinterpret_cast<uint4 *>(dst);
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
-       i < nvec; i += stride) {
-    uint4 v = s4[i];
-    if (sat_all) {
-      v = make_uint4(qmin4, qmin4, qmin4, qmin4);
-    } else {
-      v.x = evap4(v.x, floor4, delta4);
-      v.y = evap4(v.y, floor4, delta4);
-      v.z = evap4(v.z, floor4, delta4);
-      v.w = evap4(v.w, floor4, delta4);
-    }
-    d4[i] = v;
+  evap_sweep(src, dst, pv.total, pv.q_min, pv.delta);
+}
+
+// Blocks of an evaporation sweep over `total` bytes: one per kEvapUnroll *
+// kEvapThreads vectors, at most one wave (the blocks resident on all SMs at
+// once), so that large matrices are swept by a grid-stride loop.
+int evap_grid_for(unsigned long long total, int num_sms) {
+  static int resident = 0;
+  if (resident == 0) {
+    int r = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, k_evaporate_to, kEvapThreads, 0) !=
+            cudaSuccess ||
+        r < 1)
+      r = 1;
+    resident = r;
   }
-  if (blockIdx.x == 0) {
-    for (unsigned long long i = nvec * 16 + threadIdx.x; i < pv.total; i += blockDim.x) {
-      const uint8_t q = src[i];
-      dst[i] = ((int)q > fl) ? (uint8_t)(q - pv.delta) : pv.q_min;
-    }
-  }
+  const unsigned long long per_block = (unsigned long long)kEvapUnroll * kEvapThreads;
+  unsigned long long g = (total / 16 + per_block - 1) / per_block;
+  const unsigned long long cap =
+      (unsigned long long)(num_sms > 0 ? num_sms : 148) * (unsigned long long)resident;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
 }
 
 cudaError_t launch_evaporate_to(const PheromoneView &pv, uint8_t *tau_alt, DevState *st,
                                 int grid, cudaStream_t s) {
-  k_evaporate_to<<<grid, 512, 0, s>>>(pv, tau_alt, st);
+  k_evaporate_to<<<grid, kEvapThreads, 0, s>>>(pv, tau_alt, st);
   return cudaGetLastError();
 }
 
@@ -1234,40 +1286,13 @@ struct EvapArgs {
   uint8_t *tau_alt;      // second pheromone buffer of the context, or null
 };
 
-__global__ void __launch_bounds__(512) k_evap_deposit(EvapArgs a) {
+__global__ void __launch_bounds__(kEvapThreads) k_evap_deposit(EvapArgs a) {
   if (a.st) {
     if (*(volatile int *)&a.st->skip || !*(volatile int *)&a.st->found) return;
   }
   PheromoneView pv = a.pv;  // in place, on the current buffer
   pv.tau = cur_tau(a.pv.tau, a.tau_alt, a.st);
-  // q > q_min + delta ? q - delta : q_min  ==  max(q, q_min + delta) - delta
-  const int fl = (int)pv.q_min + (int)pv.delta;
-  const bool sat_all = fl > 255;
-  const uint32_t floor4 = 0x01010101u * (uint32_t)(sat_all ? 0 : fl);
-  const uint32_t delta4 = 0x01010101u * (uint32_t)pv.delta;
-  const uint32_t qmin4 = 0x01010101u * (uint32_t)pv.q_min;
-  const unsigned long long nvec = pv.total / 16;
-  uint4 *p4 = reinterpret_cast<uint4 *>(pv.tau);
-  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
-       i < nvec; i += stride) {
-    uint4 v = p4[i];
-    if (sat_all) {
-      v = make_uint4(qmin4, qmin4, qmin4, qmin4);
-    } else {
-      v.x = evap4(v.x, floor4, delta4);
-      v.y = evap4(v.y, floor4, delta4);
-      v.z = evap4(v.z, floor4, delta4);
-      v.w = evap4(v.w, floor4, delta4);
-    }
-    p4[i] = v;
-  }
-  if (blockIdx.x == 0) {
-    for (unsigned long long i = nvec * 16 + threadIdx.x; i < pv.total; i += blockDim.x) {
-      uint8_t q = pv.tau[i];
-      pv.tau[i] = ((int)q > fl) ? (uint8_t)(q - pv.delta) : pv.q_min;
-    }
-  }
+  evap_sweep(pv.tau, pv.tau, pv.total, pv.q_min, pv.delta);
   // The last block to finish the sweep deposits (threadfence reduction).
   __shared__ int s_last;
   __syncthreads();
@@ -1311,7 +1336,7 @@ cudaError_t launch_evap_deposit(const InstanceView &iv, const PheromoneView &pv,
   a.dep_iter = a.dep_global = 0.0f;
   a.tau_alt = tau_alt;
   const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
-  k_evap_deposit<<<grid, 512, smem, s>>>(a);
+  k_evap_deposit<<<grid, kEvapThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -1338,7 +1363,7 @@ cudaError_t launch_evap_deposit_explicit(const InstanceView &iv,
   a.dep_global = dep_global;
   a.tau_alt = nullptr;  // the caller passes the current buffer
   const size_t smem = iv.K <= kDepositSmemRoutes ? sizeof(int) * (iv.K + 1) : 0;
-  k_evap_deposit<<<grid, 512, smem, s>>>(a);
+  k_evap_deposit<<<grid, kEvapThreads, smem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -479,13 +479,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   // tau_min^alpha scale: 16 (1 - alpha log2 tau_min).
   ctx->et.e_dep = (int)llround(16.0 * (1.0 - p->alpha * (double)ctx->log_min / log(2.0)));
   ctx->plan = plan_construct(iv, -1, ctx->num_sms, ctx->max_smem);
-  {
-    unsigned long long nvec = tau_total / 16;
-    unsigned long long g = (nvec + 511) / 512;
-    if (g < 1) g = 1;
-    if (g > (unsigned long long)ctx->num_sms * 4) g = (unsigned long long)ctx->num_sms * 4;
-    ctx->evap_grid = (int)g;
-  }
+  ctx->evap_grid = evap_grid_for(tau_total, ctx->num_sms);
 
   TRY(launch_knn_levels(ctx->d_coords, n, k, ctx->d_thr, kThresholds, ctx->d_cand, ctx->d_lvl, s));
   TRY(launch_fill_u8(ctx->d_tau, tau_total, ctx->q_tau0, s));
@@ -736,6 +730,42 @@ int aco_b200_profile_epochs(aco_b200_ctx *ctx, int epochs, float *kernel_ms) {
     }
   }
   for (int i = 0; i < 5; ++i) cudaEventDestroy(ev[i]);
+  return rc;
+}
+
+int aco_b200_profile_update(aco_b200_ctx *ctx, int launches, float *ms_per_launch) {
+  if (!ctx || !ctx->ready || launches < 1 || !ms_per_launch) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  std::vector<cudaEvent_t> ev(2 * (size_t)launches, nullptr);
+  int rc = ACO_OK;
+  cudaError_t err = cudaSuccess;
+  for (size_t i = 0; i < ev.size() && err == cudaSuccess; ++i) err = cudaEventCreate(&ev[i]);
+  // The sweep reads the skip flag: make sure this epoch is not marked skipped.
+  if (err == cudaSuccess) err = launch_set_run_limit(ctx->d_state, 0, s);
+  ctx->run_limit_off = true;
+  if (err == cudaSuccess) err = cudaMemsetAsync(&ctx->d_state->skip, 0, sizeof(int), s);
+  for (int i = 0; i < launches && err == cudaSuccess; ++i) {
+    err = cudaEventRecord(ev[2 * i], s);
+    if (err == cudaSuccess)
+      err = launch_evaporate_to(ctx->pv, ctx->d_tau2, ctx->d_state, ctx->evap_grid, s);
+    if (err == cudaSuccess) err = cudaEventRecord(ev[2 * i + 1], s);
+  }
+  if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+  double total = 0.0;
+  for (int i = 0; i < launches && err == cudaSuccess; ++i) {
+    float ms = 0.f;
+    err = cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]);
+    total += ms;
+  }
+  if (err != cudaSuccess) {
+    fprintf(stderr, "aco_b200: profile_update failed: %s\n", cudaGetErrorString(err));
+    rc = ACO_ERR_BACKEND;
+  } else {
+    *ms_per_launch = (float)(total / launches);
+  }
+  for (cudaEvent_t e : ev)
+    if (e) cudaEventDestroy(e);
   return rc;
 }
 

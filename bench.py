@@ -1,7 +1,8 @@
 """Benchmark of the ACO-for-CVRP hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload n1000|small|clustered2000|batched|learned]
+                    [--workload n1000|small|clustered2000|large16000|large32000|
+                                batched|learned|costdist]
 
 Default workload (n1000): n=1000, K=8 uniform integer coordinates in
 [0,1000]^2 from seed 19001, depot (500,500), demands uniform in [1,100],
@@ -10,6 +11,8 @@ ACO epoch (construct all ants, iteration/global best, evaporate, deposit);
 the metric is ant-steps/s (one ant-step = one customer move or depot return).
 small: n=100, K=4, demands [1,30], seed 1001, 128 ants, 20-NN.
 clustered2000: n=2000, K=16, 70% in 8 Gaussian clusters, 1024 ants, 32-NN.
+large16000 / large32000: n=16000, K=16 / n=32000, K=32, uniform, 256 ants,
+32-NN (pheromone matrices of 256 MB / 1 GB, beyond L2).
 batched: 512 instances (n~U[50,500], K=ceil(n/60), seeds 30000-30511), 64
 ants, 16-NN, 300 epochs each, all in one persistent launch; a step is one
 solve of the whole batch and the metric is instances/s.
@@ -24,6 +27,10 @@ n=1000 instances (training set, training and evaluation inside the run).
   on the host.
 * roofline: the dominant kernel, algorithmic bytes per ant-step k(4 + 4 + 1)
   (candidate id, weight, pheromone byte) over its mean event-timed duration.
+* roofline_update: the pheromone evaporation sweep, 2 (n+1)^2 bytes per
+  launch over its mean event-timed duration, timed alone; where the
+  workload's matrices fit in L2 (n1000, small, clustered2000) the line also
+  carries roofline_update_hbm, the same sweep on an n=16000 matrix pair.
 * cli_same_contract / reference_cuda_same_gpu (reference arm): this
   library's aco_vrp_cuda.out and the reference's own CUDA solver (built from
   its sources for sm_100a) run through the same CLI on the same GPU and the
@@ -69,15 +76,25 @@ WORKLOADS = {
                   name="n100 K4 uniform seed1001 demand[1,30] 128 ants 20-NN"),
     "clustered2000": dict(factory=I.workload_clustered2000, ants=1024, cand_k=32, e2e_epochs=32,
                           name="n2000 K16 clustered seed29001 demand[1,100] 1024 ants 32-NN"),
+    "large16000": dict(factory=lambda: I.workload_large(16000), ants=256, cand_k=32, e2e_epochs=8,
+                       name="n16000 K16 uniform seed160001 demand[1,100] 256 ants 32-NN"),
+    "large32000": dict(factory=lambda: I.workload_large(32000), ants=256, cand_k=32, e2e_epochs=4,
+                       name="n32000 K32 uniform seed320001 demand[1,100] 256 ants 32-NN"),
 }
+# L2 of one B200 (bytes): a pheromone matrix pair below it stays L2-resident
+# between sweeps.
+L2_BYTES = 126 * 1024 * 1024
 BATCHED = dict(count=512, seed0=30000, ants=64, cand_k=16, epochs=300,
                name="512 instances n~U[50,500] K=ceil(n/60) seeds 30000-30511 demand[1,100] "
                     "64 ants 16-NN 300 epochs")
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_construct launch on
-# the n1000 workload (profiles/k_construct_n1000.md): the candidate tables
-# come from L2 into shared memory, so DRAM sees little of the algorithmic
-# bytes.  Other workloads report null.
+# the n1000 workload, from an ncu capture made separately (not measured in
+# this run): the candidate tables come from L2 into shared memory, so DRAM
+# sees little of the algorithmic bytes.  Other workloads report null.
 CONSTRUCT_DRAM_BYTES_PER_LAUNCH = {"n1000": 243456}
+# The same for one k_evaporate_to launch, keyed by n (ncu capture made
+# separately).
+UPDATE_DRAM_BYTES_PER_LAUNCH = {}
 OMP_BIN = os.path.join(ROOT, "oracle", "_ref", "aco_vrp_omp.out")
 REF_CUDA_BIN = os.path.join(ROOT, "oracle", "_ref", "aco_vrp_cuda_ref.out")
 SEQ_BIN = os.path.join(ROOT, "oracle", "_ref", "aco_vrp_seq.out")
@@ -185,19 +202,89 @@ def _omp_epoch_seconds(inst, ants, threads, target_s, td):
     return max((tb - ta) / epochs, 1e-9), epochs
 
 
+def omp_candidate_k(n):
+    """Candidate-list length the reference OpenMP solver picks for n on this
+    host: 0.7 L3 / ((n+1) 8 B), clamped to [16, 512], 32 when the L3 size is
+    unknown (tune_candidate_k and get_l3_cache_size,
+    src/openmp-mpi/aco_parallel.c:143-174)."""
+    l3 = 0
+    try:
+        with open("/sys/devices/system/cpu/cpu0/cache/index3/size") as f:
+            txt = f.read().strip()
+        num = int("".join(ch for ch in txt if ch.isdigit()) or 0)
+        unit = next((ch for ch in txt if ch in "KMGTkmgt"), "")
+        l3 = num * {"k": 1 << 10, "m": 1 << 20, "g": 1 << 30}.get(unit.lower(), 1)
+    except OSError:
+        pass
+    if l3 <= 0:
+        return {"k": 32, "effective_k": min(32, n), "l3_bytes": None}
+    k = max(16, min(512, int(l3 * 0.7 / ((n + 1) * 8.0))))
+    # slots past the n customers stay empty
+    return {"k": k, "effective_k": min(k, n), "l3_bytes": l3}
+
+
+def cpu_baseline_seq_construct(inst, cand_k, target_s=10.0):
+    """ant-steps/s of the reference's own sequential construction
+    (build_ant_solution, src/seq/aco_sequential.c:616-681, compiled from its
+    sources into oracle/_ref/libseqref.so) on the unit-demand twin, fed this
+    path's candidate lists and weights at the initial pheromone and recorded
+    draws.  For large n, where the reference solvers' own set-up (an
+    O(n^2 k) candidate build over a candidate list of up to 512) does not
+    finish in a bounded sample.  The distance matrix the harness builds per
+    call is excluded by timing 1 and 1 + a ants."""
+    from oracle import oracle as O
+    O.build()
+    twin = inst.unit_twin()
+    n, K = twin.n, twin.vehicles
+    A, lut, thr = O.tables()
+    cand = O.knn(twin.x, twin.y, cand_k)
+    lvl = O.levels(twin.x, twin.y, cand, cand_k, thr)
+    tau = np.full((n + 1) ** 2, O.params()["q_tau0"], np.uint8)
+    w = O.weights(n, cand_k, cand, lvl, tau, A, lut)
+    rs = np.random.RandomState(7)
+
+    def run(m):
+        dr = rs.randint(0, 1 << 24, size=(m, n + K + 8)).astype(np.uint32)
+        t0 = time.perf_counter()
+        res = O.ref_construct_ants(twin.x, twin.y, K, twin.capacity, cand_k, cand, w, dr)
+        return time.perf_counter() - t0, sum(int(r[1].sum()) - K for r in res)
+
+    t1, s1 = run(1)
+    extra = 2
+    while True:
+        t2, s2 = run(1 + extra)
+        if t2 - t1 > target_s / 4 or extra >= 64:
+            break
+        extra *= 2
+    per_step = max(t2 - t1, 1e-9) / max(s2 - s1, 1)
+    return {"value": 1.0 / per_step, "unit": "ant-steps/s", "cores": 1, "kind": "reference",
+            "sample": (f"the reference's sequential build_ant_solution (compiled from its "
+                       f"sources) on the unit-demand twin, {extra} ants with recorded draws on "
+                       f"this path's {cand_k}-NN lists and initial weights, one thread; the "
+                       "reference solvers' own set-up is O(n^2 k) and does not finish in a "
+                       "bounded sample at this n")}
+
+
 def cpu_baseline(inst, ants, target_s=12.0, cand_k=32):
     """ant-steps/s of the reference's own CPU path, bounded sample."""
     n, K = inst.n, inst.vehicles
-    steps_per_epoch = ants * (n + K)
+    if n > 4000:
+        from oracle import oracle as O
+        if O.ref_available():
+            return cpu_baseline_seq_construct(inst, cand_k)
     if os.path.exists(OMP_BIN):
         threads = os.cpu_count() or 1
+        steps_per_epoch = ants * (n + K)
         with tempfile.TemporaryDirectory() as td:
             per_epoch, epochs = _omp_epoch_seconds(inst, ants, threads, target_s, td)
+        kc = omp_candidate_k(n)
         return {"value": steps_per_epoch / per_epoch, "unit": "ant-steps/s", "cores": threads,
-                "kind": "reference",
+                "kind": "reference", "candidate_k": kc,
                 "sample": (f"reference OpenMP solver (aco_parallel.c, no MPI) on the unit-demand "
                            f"twin, {ants} ants, {epochs} fixed epochs minus a 2-epoch run "
-                           f"(set-up excluded), OMP_NUM_THREADS={threads}")}
+                           f"(set-up excluded), OMP_NUM_THREADS={threads}, its own L3-tuned "
+                           f"candidate list of {kc['k']} (this GPU path uses {cand_k})")}
+    steps_per_epoch = ants * (n + K)
     # Fallback: the oracle port, one thread, one epoch of `ants` ants.
     from oracle import oracle as O
     O.build()
@@ -304,7 +391,7 @@ def run_reference_arm(args, rank, world):
                     "d2h_bytes_per_step": 0}}
     if ref_gpu is not None:
         line["reference_cuda_same_gpu"] = ref_gpu
-    if args.workload != "batched" and os.path.exists(SEQ_BIN):
+    if args.workload != "batched" and inst.n <= 4000 and os.path.exists(SEQ_BIN):
         # The reference's sequential solver on one host core, same CLI.
         try:
             line["reference_seq_1core"] = cli_epoch_rate(SEQ_BIN, inst, wl["ants"], seconds=10.0)
@@ -317,6 +404,26 @@ def run_reference_arm(args, rank, world):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+
+def update_roofline(ctx, n, launches, peak, peak_kind):
+    """Roofline of the pheromone evaporation sweep (k_evaporate_to, the
+    reference's kernel_evaporate_tau) on this context's matrix: 2 (n+1)^2
+    algorithmic bytes (each byte read once and written once) per launch over
+    the mean CUDA-event time of one launch, the sweep timed alone."""
+    ms = ctx.profile_update(launches)
+    nbytes = 2 * (n + 1) ** 2
+    achieved = nbytes / (ms / 1e3) / 1e9
+    resident = nbytes <= L2_BYTES
+    return {"bound": "hbm", "kernel": "k_evaporate_to", "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "n": n,
+            "bytes_per_launch": nbytes, "us_per_launch": ms * 1e3, "launches": launches,
+            "residency": ("L2-resident: both matrices fit in L2, so this is not an HBM figure"
+                          if resident else "HBM: the matrices exceed L2"),
+            "traffic": UPDATE_DRAM_BYTES_PER_LAUNCH.get(n),
+            "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                               "captured separately" if n in UPDATE_DRAM_BYTES_PER_LAUNCH
+                               else None)}
+
 
 def timed_steps(torch, stream, steps, enqueue, flush):
     """Device ms of `steps` calls of enqueue(), each bracketed by events, the
@@ -361,6 +468,17 @@ def run_single(args, rank, world, local, torch, dist, _native):
     steps_done = st.total_steps - steps0
     assert st.error == 0 and st.epochs == args.warmup + args.steps
     kms = ctx.profile_epochs(32) / 32.0
+    peak, peak_kind = load_peaks()
+    roof_upd = update_roofline(ctx, n, 200 if n <= 4000 else 50, peak, peak_kind)
+    roof_upd_hbm = None
+    if rank == 0 and (n + 1) ** 2 * 2 <= L2_BYTES and not args.no_large_update:
+        # The matrix of this workload stays in L2; the same sweep on an
+        # n=16000 matrix pair (512 MB) gives the HBM figure.
+        with _native.Context(local) as cl:
+            big = I.workload_large(16000)
+            cl.set_stream(stream.cuda_stream)
+            cl.setup_instance(big, ants=32, cand_k=k, seed=5)
+            roof_upd_hbm = update_roofline(cl, big.n, 50, peak, peak_kind)
     t = torch.tensor([dev_ms, float(steps_done)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
@@ -391,7 +509,6 @@ def run_single(args, rank, world, local, torch, dist, _native):
         dist.all_reduce(te, op=dist.ReduceOp.SUM)
         e2e = float(te[0])
 
-    peak, peak_kind = load_peaks()
     bytes_per_step = k * (4 + 4 + 1)
     achieved = bytes_per_step * (steps_done / args.steps) / (float(kms[1]) / 1e3) / 1e9
     total_k = float(kms.sum())
@@ -419,7 +536,11 @@ def run_single(args, rank, world, local, torch, dist, _native):
                          "frac": achieved / peak,
                          "traffic": CONSTRUCT_DRAM_BYTES_PER_LAUNCH.get(args.workload),
                          "kernel": "k_construct", "peak_kind": peak_kind,
-                         "bytes_per_ant_step": bytes_per_step},
+                         "bytes_per_ant_step": bytes_per_step,
+                         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                            "of one launch, captured separately")
+                         if args.workload in CONSTRUCT_DRAM_BYTES_PER_LAUNCH else None},
+            "roofline_update": roof_upd,
             "e2e": {"value": e2e, "unit": "ant-steps/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "step": f"one solve through the C ABI on a reused context: upload, "
@@ -427,6 +548,8 @@ def run_single(args, rank, world, local, torch, dist, _native):
                             "routes"},
             "clocks": clk.summary(),
         }
+        if roof_upd_hbm is not None:
+            line["roofline_update_hbm"] = roof_upd_hbm
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(inst, m, cand_k=k)
@@ -774,6 +897,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--looped-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-large-update", action="store_true",
+                    help="skip the n=16000 pheromone-sweep roofline of small workloads")
     ap.add_argument("--no-cli", dest="cli", action="store_false",
                     help="skip the drop-in CLI timing on the unit-demand twin")
     ap.add_argument("--colony", default="auto", choices=["auto", "sharded"],

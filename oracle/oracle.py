@@ -80,6 +80,9 @@ def ref():
         vp, i32 = C.c_void_p, C.c_int
         R.seqref_construct_ant.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, vp, i32, vp, vp, vp]
         R.seqref_construct_ant.restype = i32
+        R.seqref_construct_ants.argtypes = [i32, i32, i32, i32, vp, vp, vp, vp, i32, vp, i32,
+                                            vp, vp, vp, vp]
+        R.seqref_construct_ants.restype = i32
         R.seqref_solution_cost.argtypes = [i32, i32, vp, vp, vp, vp]
         R.seqref_solution_cost.restype = C.c_double
         R.seqref_validate.argtypes = [i32, i32, vp, vp]
@@ -216,6 +219,28 @@ def deposit(tau: np.ndarray, n, nodes, lens, dep, log_min, log_step, q_min=0,
 # --------------------------------------------------------------------------
 # The reference's own code (oracle/_ref), when built.
 # --------------------------------------------------------------------------
+
+def ref_construct_ants(x, y, K, cap, k, cand, w, draw_streams):
+    """The reference's build_ant_solution for every row of draw_streams
+    (m x n_draws recorded draws), one distance matrix for all ants.
+    Returns [(nodes, lens, cost, used)] per ant."""
+    n = len(x) - 1
+    d = np.ascontiguousarray(draw_streams, np.uint32)
+    m, nd = d.shape
+    nodes = np.zeros((m, n + 2 * K), dtype=np.int32)
+    lens = np.zeros((m, K), dtype=np.int32)
+    cost = np.zeros(m, dtype=np.float64)
+    used = np.zeros(m, dtype=np.int32)
+    rc = ref().seqref_construct_ants(
+        n, K, int(cap), k, _p(np.ascontiguousarray(x, np.float32)),
+        _p(np.ascontiguousarray(y, np.float32)), _p(np.ascontiguousarray(cand, np.int32)),
+        _p(np.ascontiguousarray(w, np.uint32)), m, _p(d), nd, _p(nodes), _p(lens), _p(cost),
+        _p(used))
+    if rc < 0:
+        raise RuntimeError(f"seqref_construct_ants failed ({rc})")
+    return [(nodes[a, : int(lens[a].sum())].copy(), lens[a].copy(), float(cost[a]),
+             int(used[a])) for a in range(m)]
+
 
 def ref_construct_ant(x, y, K, cap, k, cand, w, draw_stream):
     n = len(x) - 1

@@ -48,17 +48,20 @@ static double **harness_matrix(int n, const float *x, const float *y) {
 }
 
 /*
- * Builds one ant with the reference code.  Returns the number of draws used,
- * or -1 on allocation failure, -2 if the recorded stream ran out.  Routes are
- * written in compact form (K segments [0 ... 0] back to back, capacity
- * n + 2K) with the K lengths; cost_out is the reference's solution_cost.
+ * Builds m ants with the reference code over one distance matrix (built once
+ * per call; at n=8000 it is 512 MB).  Ant a pops the recorded stream
+ * draws[a * n_draws .. (a+1) * n_draws).  Returns 0, -1 on allocation
+ * failure, -2 if a recorded stream ran out.  Ant a's routes are written in
+ * compact form (K segments [0 ... 0] back to back) at nodes_out + a (n + 2K),
+ * its K lengths at lens_out + a K, the reference's solution_cost at
+ * cost_out[a] and the number of draws it used at used_out[a].
  */
 __attribute__((visibility("default")))
-int seqref_construct_ant(int n, int K, int cap, int k, const float *x,
-                         const float *y, const int32_t *cand,
-                         const uint32_t *w, const uint32_t *draws,
-                         int n_draws, int32_t *nodes_out, int32_t *lens_out,
-                         double *cost_out) {
+int seqref_construct_ants(int n, int K, int cap, int k, const float *x,
+                          const float *y, const int32_t *cand,
+                          const uint32_t *w, int m, const uint32_t *draws,
+                          int n_draws, int32_t *nodes_out, int32_t *lens_out,
+                          double *cost_out, int32_t *used_out) {
   SeqShared shared;
   memset(&shared, 0, sizeof(shared));
   shared.n = n;
@@ -70,12 +73,7 @@ int seqref_construct_ant(int n, int K, int cap, int k, const float *x,
   shared.eta_beta = (float *)calloc(elems, sizeof(float));
   shared.score = (float *)calloc(elems, sizeof(float));
   double **c = harness_matrix(n, x, y);
-  SeqWorkspace ws;
-  int ws_ok = 0;
-  if (shared.candidate_idx && shared.eta_beta && shared.score && c) {
-    ws_ok = seq_workspace_init(&ws, K, n, shared.visited_words);
-  }
-  if (!ws_ok) {
+  if (!shared.candidate_idx || !shared.eta_beta || !shared.score || !c) {
     free(shared.candidate_idx);
     free(shared.eta_beta);
     free(shared.score);
@@ -86,31 +84,51 @@ int seqref_construct_ant(int n, int K, int cap, int k, const float *x,
     shared.candidate_idx[e] = cand[e];
     shared.score[e] = (float)w[e];
   }
-
-  g_draws = draws;
-  g_n_draws = n_draws;
-  g_next_draw = 0;
-  g_overflow = 0;
-
-  build_ant_solution(&ws, &shared, K, cap < 1 ? 1 : cap, c);
-  *cost_out = solution_cost(ws.sol, c);
-
-  int off = 0;
-  for (int v = 0; v < K; ++v) {
-    const Route *r = &ws.sol->routes[v];
-    for (int t = 0; t < r->len; ++t) nodes_out[off + t] = r->nodes[t];
-    lens_out[v] = r->len;
-    off += r->len;
+  int rc = 0;
+  for (int a = 0; a < m && rc == 0; ++a) {
+    SeqWorkspace ws;
+    if (!seq_workspace_init(&ws, K, n, shared.visited_words)) {
+      rc = -1;
+      break;
+    }
+    g_draws = draws + (size_t)a * (size_t)n_draws;
+    g_n_draws = n_draws;
+    g_next_draw = 0;
+    g_overflow = 0;
+    build_ant_solution(&ws, &shared, K, cap < 1 ? 1 : cap, c);
+    cost_out[a] = solution_cost(ws.sol, c);
+    int32_t *nodes = nodes_out + (size_t)a * (size_t)(n + 2 * K);
+    int off = 0;
+    for (int v = 0; v < K; ++v) {
+      const Route *r = &ws.sol->routes[v];
+      for (int t = 0; t < r->len; ++t) nodes[off + t] = r->nodes[t];
+      lens_out[(size_t)a * K + v] = r->len;
+      off += r->len;
+    }
+    used_out[a] = g_next_draw;
+    if (g_overflow) rc = -2;
+    seq_workspace_free(&ws);
   }
-  int used = g_next_draw;
-  int overflow = g_overflow;
-
-  seq_workspace_free(&ws);
   free(shared.candidate_idx);
   free(shared.eta_beta);
   free(shared.score);
   matrix_free(c);
-  return overflow ? -2 : used;
+  return rc;
+}
+
+/* One ant (seqref_construct_ants with m = 1).  Returns the number of draws
+ * used, or -1 on allocation failure, -2 if the recorded stream ran out;
+ * cost_out is the reference's solution_cost. */
+__attribute__((visibility("default")))
+int seqref_construct_ant(int n, int K, int cap, int k, const float *x,
+                         const float *y, const int32_t *cand,
+                         const uint32_t *w, const uint32_t *draws,
+                         int n_draws, int32_t *nodes_out, int32_t *lens_out,
+                         double *cost_out) {
+  int32_t used = 0;
+  const int rc = seqref_construct_ants(n, K, cap, k, x, y, cand, w, 1, draws, n_draws,
+                                       nodes_out, lens_out, cost_out, &used);
+  return rc < 0 ? rc : used;
 }
 
 /* The reference's FP64 cost of a route set in compact form

@@ -147,6 +147,14 @@ def workload_clustered2000(seed: int = 29001) -> Instance:
                               name=f"c3_n2000_k16_s{seed}")
 
 
+def workload_large(n: int = 16000) -> Instance:
+    """Large uniform instance in the reference's published CUDA size range
+    (n = 4000-64000): K = n / 1000 vehicles, demands [1,100], seed 10 n + 1
+    (n=16000: tau is 256 MB; n=32000: 1 GB; 256 ants, 32-NN)."""
+    K = max(1, n // 1000)
+    return uniform_instance(n, K, 10 * n + 1, demand_max=100, name=f"large_n{n}_k{K}")
+
+
 def prior_training_instances(count: int = 4096, seed0: int = 40000) -> List[Instance]:
     """Training set of the learned prior: n ~ U[200,1000] (drawn from seed0),
     K = ceil(n/125), demands [1,100]; even indices uniform, odd clustered;

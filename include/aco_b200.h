@@ -133,6 +133,12 @@ ACO_API int aco_b200_get_best(aco_b200_ctx *ctx, int *nodes, int *lens, double *
 
 ACO_API int aco_b200_get_state(aco_b200_ctx *ctx, aco_b200_state *state);
 ACO_API int aco_b200_get_dims(aco_b200_ctx *ctx, int *n, int *K, int *k, int *m);
+/* Launch shape of the construction chosen at set-up: out[0] ants (warps)
+ * per block, out[1] table layout (0 weights staged in shared memory, 1
+ * packed levels staged, 2 rows read from global memory), out[2] visited
+ * bitmap words per lane held in registers (0: bitmap in shared memory),
+ * out[3] dynamic shared memory per block in bytes. */
+ACO_API int aco_b200_get_plan(aco_b200_ctx *ctx, int out[4]);
 
 /* Test hooks (parity checks against the oracle). */
 ACO_API int aco_b200_get_tau(aco_b200_ctx *ctx, uint8_t *tau);       /* (n+1)^2 */

@@ -42,7 +42,15 @@ CASES = {
     "u3000_demand": (lambda: I.uniform_instance(3000, 24, 604), 32, 32),
     # K > 4096 routes of one or two customers: the deposit's unstaged path
     "many_vehicles": (lambda: I.Instance("mv", *_many_vehicles()), 8, 8),
+    # the clustered n=2000 workload as benched: 1024 ants, 7 ants per block,
+    # packed levels in shared memory
+    "c3_bench": (I.workload_clustered2000, 32, 1024),
+    # n=16000: visited bitmap in shared memory, rows from global memory, in
+    # the reference's published CUDA size range
+    "u16000_unit": (lambda: I.uniform_instance(16000, 16, 660).unit_twin(), 32, 16),
 }
+# Cases checked on every STRIDE-th ant only (the oracle is sequential).
+STRIDE = {"c3_bench": 8}
 
 
 def _many_vehicles():
@@ -130,16 +138,30 @@ def check_construct(O, inst, ctx, seed, epoch, tau, ants=None):
 
 @pytest.mark.parametrize("name", ["smoke", "u200_unit", "small_c1", "u300_demand", "n1000_c2",
                                   "n1000_unit", "c2000_demand", "u3000_demand",
-                                  "many_vehicles"])
+                                  "many_vehicles", "c3_bench", "u16000_unit"])
 def test_construct_matches_oracle(oracle_mod, name):
     factory, k, m = CASES[name]
     inst = factory()
+    ants = range(0, m, STRIDE.get(name, 1))
     with make_ctx(inst, k, m, seed=4321) as ctx:
         for epoch, mode in [(0, None), (3, "random"), (9, "mostly_init")]:
             tau = ctx.tau() if mode is None else random_tau(inst.n, epoch, mode)
             ctx.set_tau(tau)
             ctx.construct(epoch)
-            check_construct(oracle_mod, inst, ctx, 4321, epoch, tau)
+            check_construct(oracle_mod, inst, ctx, 4321, epoch, tau, ants=ants)
+
+
+def test_benched_shapes_take_the_tested_plans():
+    """The launch shapes the parity cases above stand for: the clustered
+    n=2000 workload as benched runs 7 ants per block on packed levels in
+    shared memory, n=16000 reads rows from global memory with the visited
+    bitmap in shared memory."""
+    with make_ctx(I.workload_clustered2000(), 32, 1024) as ctx:
+        plan = ctx.plan()
+        assert plan["wpb"] == 7 and plan["layout"] == _native.LAYOUT_SMEM_PACKED
+    with make_ctx(CASES["u16000_unit"][0](), 32, 16) as ctx:
+        plan = ctx.plan()
+        assert plan["layout"] == _native.LAYOUT_GLOBAL and plan["vreg"] == 0
 
 
 @pytest.mark.parametrize("layout", [_native.LAYOUT_SMEM_WEIGHTS, _native.LAYOUT_SMEM_PACKED,
@@ -421,7 +443,8 @@ def test_setup_reuse_matches_fresh_contexts():
                 assert bc == fc and np.array_equal(bn, fn) and np.array_equal(bl, fl)
 
 
-@pytest.mark.parametrize("n", [400, 1500, 3000])  # staged weights, packed levels, global rows
+# staged weights, packed levels, global rows; n=8000 with the bitmap in shared memory
+@pytest.mark.parametrize("n", [400, 1500, 3000, 8000])
 def test_recorded_draws_match_reference_seq_code(oracle_mod, n):
     """The harness of the parity contract: the GPU construction and the
     reference's own build_ant_solution (src/seq/aco_sequential.c:616-681,
@@ -441,9 +464,9 @@ def test_recorded_draws_match_reference_seq_code(oracle_mod, n):
         cand, lvl = ctx.candidates()
         A, lut, _ = O.tables()
         w = O.weights(inst.n, k, cand, lvl, ctx.tau(), A, lut)
-        for a in range(m):
-            rn, rl, rc, ru = O.ref_construct_ant(inst.x, inst.y, inst.vehicles, inst.capacity,
-                                                 k, cand, w, draws[a])
+        refs = O.ref_construct_ants(inst.x, inst.y, inst.vehicles, inst.capacity, k, cand, w,
+                                    draws)
+        for a, (rn, rl, rc, ru) in enumerate(refs):
             assert np.array_equal(lens[a], rl) and np.array_equal(nodes[a][: rl.sum()], rn)
             assert abs(cost[a] - rc) <= 1e-9 * rc and used[a] == ru
         # Philox draws recorded and replayed give the Philox run's routes

@@ -28,7 +28,7 @@ N_THRESHOLDS = 4095
 EXPORTED = [
     "aco_b200_create", "aco_b200_destroy", "aco_b200_set_stream", "aco_b200_setup",
     "aco_b200_run", "aco_b200_enqueue_epochs", "aco_b200_synchronize",
-    "aco_b200_get_best", "aco_b200_get_state", "aco_b200_get_dims",
+    "aco_b200_get_best", "aco_b200_get_state", "aco_b200_get_dims", "aco_b200_get_plan",
     "aco_b200_get_tau", "aco_b200_set_tau", "aco_b200_get_candidates",
     "aco_b200_get_tables", "aco_b200_get_weights", "aco_b200_construct",
     "aco_b200_get_ants", "aco_b200_evaporate_deposit", "aco_b200_build_info",
@@ -118,7 +118,7 @@ def load():
         "aco_b200_run": [vp, i32, vp, vp, i32, vp],
         "aco_b200_enqueue_epochs": [vp, i32], "aco_b200_synchronize": [vp],
         "aco_b200_get_best": [vp, vp, vp, vp], "aco_b200_get_state": [vp, vp],
-        "aco_b200_get_dims": [vp, vp, vp, vp, vp],
+        "aco_b200_get_dims": [vp, vp, vp, vp, vp], "aco_b200_get_plan": [vp, vp],
         "aco_b200_get_tau": [vp, vp], "aco_b200_set_tau": [vp, vp],
         "aco_b200_get_candidates": [vp, vp, vp],
         "aco_b200_get_tables": [vp, vp, vp, vp, i32],
@@ -229,6 +229,14 @@ class Context:
                                             C.byref(m)), "aco_b200_get_dims")
         self.n, self.K, self.k, self.m = n.value, K_.value, k.value, m.value
         return self
+
+    def plan(self) -> dict:
+        """Launch shape of the construction (ants per block, table layout,
+        register bitmap words per lane, shared memory bytes)."""
+        out = np.zeros(4, np.int32)
+        _check(self._lib.aco_b200_get_plan(self._h, _p(out)), "aco_b200_get_plan")
+        return {"wpb": int(out[0]), "layout": int(out[1]), "vreg": int(out[2]),
+                "smem": int(out[3])}
 
     def setup_instance(self, inst, **kw):
         demand = None if inst.is_unit_demand() else inst.demand

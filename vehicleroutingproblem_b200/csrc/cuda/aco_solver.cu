@@ -794,6 +794,15 @@ int aco_b200_get_dims(aco_b200_ctx *ctx, int *n, int *K, int *k, int *m) {
   return ACO_OK;
 }
 
+int aco_b200_get_plan(aco_b200_ctx *ctx, int out[4]) {
+  if (!ctx || !ctx->ready || !out) return ACO_ERR_INVALID_INPUT;
+  out[0] = ctx->plan.wpb;
+  out[1] = ctx->plan.layout;
+  out[2] = ctx->plan.vreg;
+  out[3] = (int)ctx->plan.total;
+  return ACO_OK;
+}
+
 int aco_b200_get_best(aco_b200_ctx *ctx, int *nodes, int *lens, double *cost) {
   if (!ctx || !ctx->ready) return ACO_ERR_INVALID_INPUT;
   cudaSetDevice(ctx->device);

@@ -14,8 +14,10 @@ clustered2000: n=2000, K=16, 70% in 8 Gaussian clusters, 1024 ants, 32-NN.
 large16000 / large32000: n=16000, K=16 / n=32000, K=32, uniform, 256 ants,
 32-NN (pheromone matrices of 256 MB / 1 GB, beyond L2).
 batched: 512 instances (n~U[50,500], K=ceil(n/60), seeds 30000-30511), 64
-ants, 16-NN, 300 epochs each, all in one persistent launch; a step is one
-solve of the whole batch and the metric is instances/s.
+ants, 300 epochs each, all in one persistent launch; the autotuner chooses
+the candidate-list length (16, 20 or 32: the fastest within 0.5 % of the
+best mean final cost) and the launch shape; a step is one solve of the
+whole batch and the metric is instances/s.
 learned: the learned prior's time-to-cost against plain eta on 256 held-out
 n=1000 instances (training set, training and evaluation inside the run).
 
@@ -31,6 +33,12 @@ n=1000 instances (training set, training and evaluation inside the run).
   launch over its mean event-timed duration, timed alone; where the
   workload's matrices fit in L2 (n1000, small, clustered2000) the line also
   carries roofline_update_hbm, the same sweep on an n=16000 matrix pair.
+* batched / learned_time_to_cost (default n1000 run only, --no-extras skips
+  them): the other two figures of the headline metric -- instances/s of the
+  batched form on the full 512-instance batch beside the single-instance
+  solver looped over a sample, and the learned prior's time-to-cost against
+  plain eta (and a tuned-beta control) with 512 training and 8 held-out
+  instances.
 * cli_same_contract / reference_cuda_same_gpu (reference arm): this
   library's aco_vrp_cuda.out and the reference's own CUDA solver (built from
   its sources for sm_100a) run through the same CLI on the same GPU and the
@@ -86,7 +94,7 @@ WORKLOADS = {
 L2_BYTES = 126 * 1024 * 1024
 BATCHED = dict(count=512, seed0=30000, ants=64, cand_k=16, epochs=300,
                name="512 instances n~U[50,500] K=ceil(n/60) seeds 30000-30511 demand[1,100] "
-                    "64 ants 16-NN 300 epochs")
+                    "64 ants, candidate lists of 16/20/32 chosen by the autotuner, 300 epochs")
 # dram__bytes_read.sum + dram__bytes_write.sum of one k_construct launch on
 # the n1000 workload, from an ncu capture made separately (not measured in
 # this run): the candidate tables come from L2 into shared memory, so DRAM
@@ -550,6 +558,8 @@ def run_single(args, rank, world, local, torch, dist, _native):
         }
         if roof_upd_hbm is not None:
             line["roofline_update_hbm"] = roof_upd_hbm
+        if world == 1 and args.workload == "n1000" and not args.no_extras:
+            line.update(default_extras(local, torch, _native))
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(inst, m, cand_k=k)
@@ -670,40 +680,40 @@ def run_sharded(args, rank, world, local, torch, dist, _native):
     return line
 
 
-def run_batched(args, rank, world, local, torch, dist, _native):
-    insts_all = I.batched_instances(BATCHED["count"], BATCHED["seed0"])
-    mine = list(range(rank, len(insts_all), world))  # this rank's slice
-    insts = [insts_all[i] for i in mine]
+def batched_measure(torch, local, _native, insts, seed0, steps, warmup, e2e_steps,
+                    looped_sample, dist=None, world=1):
+    """The batched solver on `insts` (instance i solved with seed seed0 + i):
+    autotuned candidate length and shape, `steps` solves timed with CUDA
+    events on one stream (L2 flushed between them), the end-to-end rate
+    through the C ABI with host buffers on one reused batch object, and the
+    single-instance solver looped over a sample of the same instances
+    (scaled by n + K)."""
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     b = _native.Batch(local)
     b.set_stream(stream.cuda_stream)
-    b.setup(insts, ants=BATCHED["ants"], cand_k=BATCHED["cand_k"], seed=BATCHED["seed0"],
+    b.setup(insts, ants=BATCHED["ants"], cand_k=BATCHED["cand_k"], seed=seed0,
             epochs=BATCHED["epochs"])
-    chosen, trials = b.autotune(trial_epochs=3)
-    for _ in range(args.warmup):
+    # The autotuner picks the candidate-list length (fastest within 0.5 % of
+    # the best mean final cost), then the launch shape.
+    k, chosen, per_k, trials = b.autotune_k(ks=(16, 20, 32), quality_tol=0.005, trial_epochs=3)
+    for _ in range(warmup):
         b.enqueue()
     torch.cuda.synchronize()
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
-    if world > 1:
+    if dist is not None and world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         wall0 = time.perf_counter()
-        dev_ms = timed_steps(torch, stream, args.steps, b.enqueue, flush)
+        dev_ms = timed_steps(torch, stream, steps, b.enqueue, flush)
         wall = time.perf_counter() - wall0
-    if world > 1:
+    if dist is not None and world > 1:
         dist.barrier()
-    costs, epochs, steps = b.costs()
+    costs, epochs, ant_steps = b.costs()
     assert np.all(epochs == BATCHED["epochs"])
-    t = torch.tensor([dev_ms, float(len(insts)), float(steps.sum())], dtype=torch.float64,
-                     device="cuda")
-    if world > 1:
-        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:3], op=dist.ReduceOp.SUM)
-    dev_ms_max, count_all, steps_all = float(t[0]), float(t[1]), float(t[2])
-    value = count_all * args.steps / (dev_ms_max / 1e3)
-    ant_steps_s = steps_all * args.steps / (dev_ms_max / 1e3)
+    b.close()
+    del flush
 
     # End to end through the C ABI with host buffers, as a service solving a
     # stream of batches on one batch object: set-up (upload, k-NN; the
@@ -711,10 +721,10 @@ def run_batched(args, rank, world, local, torch, dist, _native):
     # of every cost and best route.
     e2e_vals = []
     with _native.Batch(local) as b2:
-        for i in range(args.e2e_steps):
+        for i in range(e2e_steps):
             t0 = time.perf_counter()
-            b2.setup(insts, ants=BATCHED["ants"], cand_k=BATCHED["cand_k"],
-                     seed=BATCHED["seed0"], epochs=BATCHED["epochs"])
+            b2.setup(insts, ants=BATCHED["ants"], cand_k=k, seed=seed0,
+                     epochs=BATCHED["epochs"])
             b2.set_tuning(*chosen)
             b2.solve()
             res = b2.best_all()
@@ -722,29 +732,15 @@ def run_batched(args, rank, world, local, torch, dist, _native):
             assert len(res) == len(insts)
             if i > 0:
                 e2e_vals.append(len(insts) / dt)
-    e2e = statistics.median(e2e_vals) if e2e_vals else None
-    if world > 1:
-        te = torch.tensor([e2e or 0.0], dtype=torch.float64, device="cuda")
-        dist.all_reduce(te, op=dist.ReduceOp.SUM)
-        e2e = float(te[0])
-    # Bytes copied per e2e step: coordinates (8 B) and demands (4 B) per node,
-    # an 80-byte descriptor, row offset and size (12 B) and two queue orders
-    # (8 B) per instance, the level and weight tables (256 + 256 ints) and the
-    # 4095 eta thresholds up; every best route slot (n + 2K ints), the route
-    # lengths (K ints) and the costs (8 B) down.
-    nodes = sum(x.n + 1 for x in insts)
-    h2d = nodes * 12 + len(insts) * (80 + 12 + 8) + 2048 + 4095 * 4
-    d2h = sum((x.n + 2 * x.vehicles) * 4 + x.vehicles * 4 + 8 for x in insts)
-
     # Looping the single-instance solver over a sample, scaled by work.
     looped = None
-    if rank == 0 and args.looped_sample > 0:
-        sample = list(range(0, len(insts), max(1, len(insts) // args.looped_sample)))
+    if looped_sample > 0:
+        sample = list(range(0, len(insts), max(1, len(insts) // looped_sample)))
         t0 = time.perf_counter()
         for i in sample:
             with _native.Context(local) as ctx:
-                ctx.setup_instance(insts[i], ants=BATCHED["ants"], cand_k=BATCHED["cand_k"],
-                                   seed=BATCHED["seed0"] + mine[i], fixed_epochs=BATCHED["epochs"])
+                ctx.setup_instance(insts[i], ants=BATCHED["ants"], cand_k=k,
+                                   seed=seed0 + i, fixed_epochs=BATCHED["epochs"])
                 ctx.run(BATCHED["epochs"])
                 ctx.best()
         ts = time.perf_counter() - t0
@@ -752,43 +748,87 @@ def run_batched(args, rank, world, local, torch, dist, _native):
         t_all = ts * w.sum() / w[sample].sum()
         looped = {"value": len(insts) / t_all, "unit": "instances/s",
                   "sample": f"{len(sample)} instances solved one after another with the "
-                            "single-instance C ABI (300 epochs each), scaled by n+K"}
-    line = None
-    if rank == 0:
-        peak, peak_kind = load_peaks()
-        bytes_per_step = BATCHED["cand_k"] * (4 + 4 + 1)
-        achieved = bytes_per_step * ant_steps_s / 1e9
-        line = {
-            "metric": "instances/s", "value": value, "unit": "instances/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None,
-            "dtype": "int32 weights + u8 pheromone (f64 route costs)", "data": "synthetic",
-            "config": {"workload": BATCHED["name"], "instances": BATCHED["count"],
-                       "step": "one solve of the whole batch (one persistent launch)",
-                       "tuning": {"lanes_per_ant": chosen[0], "ants_per_block": chosen[1],
-                                  "order": "largest first" if chosen[2] else "as given"},
-                       "autotune_trial_ms": [round(float(x), 3) for x in trials],
-                       "l2": "flushed between timed steps (256 MiB write outside the events)",
-                       "parallelism": f"instances split over {world} GPUs" if world > 1 else "1 GPU"},
-            "ant_steps_per_s": ant_steps_s,
-            "wall_s": wall, "gpu_launches": args.steps,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "kernel": "k_batch_solve",
-                         "peak_kind": peak_kind, "bytes_per_ant_step": bytes_per_step},
-            "e2e": {"value": e2e, "unit": "instances/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h,
-                    "step": "set-up of the batch through the C ABI, one solve, download of "
-                            "every cost and best route"},
-            "looped_single_instance": looped,
-            "clocks": clk.summary(),
-        }
-        if world == 1 and not args.no_cpu_baseline:
-            try:
-                line["cpu_baseline"] = cpu_baseline_batched(insts)
-            except Exception as exc:
-                line["cpu_baseline"] = {"error": str(exc)[:200]}
-    b.close()
+                            "single-instance C ABI (300 epochs each, set-up and download "
+                            "included), scaled by n+K"}
+    per_k = {str(kk): {"solve_ms": v[0], "instances_per_s": len(insts) / (v[0] / 1e3),
+                       "mean_final_cost": v[1], "solved": v[2]} for kk, v in per_k.items()}
+    return {"dev_ms": dev_ms, "wall": wall, "clk": clk.summary(), "chosen": chosen,
+            "cand_k": k, "per_k": per_k, "trials": trials, "count": len(insts),
+            "ant_steps": float(ant_steps.sum()),
+            "mean_cost": float(np.mean(costs[costs < 1e300])) if np.any(costs < 1e300) else None,
+            "e2e": statistics.median(e2e_vals) if e2e_vals else None, "looped": looped}
+
+
+def batched_h2d_d2h(insts):
+    """Bytes copied per end-to-end batched step: coordinates (8 B) and
+    demands (4 B) per node, an 80-byte descriptor, row offset and size
+    (12 B) and two queue orders (8 B) per instance, the level and weight
+    tables (256 + 256 ints) and the 4095 eta thresholds up; every best route
+    slot (n + 2K ints), the route lengths (K ints) and the costs (8 B) down."""
+    nodes = sum(x.n + 1 for x in insts)
+    h2d = nodes * 12 + len(insts) * (80 + 12 + 8) + 2048 + 4095 * 4
+    d2h = sum((x.n + 2 * x.vehicles) * 4 + x.vehicles * 4 + 8 for x in insts)
+    return h2d, d2h
+
+
+def run_batched(args, rank, world, local, torch, dist, _native):
+    insts_all = I.batched_instances(BATCHED["count"], BATCHED["seed0"])
+    mine = list(range(rank, len(insts_all), world))  # this rank's slice
+    insts = [insts_all[i] for i in mine]
+    r = batched_measure(torch, local, _native, insts, BATCHED["seed0"], args.steps, args.warmup,
+                        args.e2e_steps, args.looped_sample if rank == 0 else 0, dist, world)
+    t = torch.tensor([r["dev_ms"], float(len(insts)), r["ant_steps"]], dtype=torch.float64,
+                     device="cuda")
+    if world > 1:
+        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:3], op=dist.ReduceOp.SUM)
+    dev_ms_max, count_all, steps_all = float(t[0]), float(t[1]), float(t[2])
+    value = count_all * args.steps / (dev_ms_max / 1e3)
+    ant_steps_s = steps_all * args.steps / (dev_ms_max / 1e3)
+    e2e = r["e2e"]
+    if world > 1:
+        te = torch.tensor([e2e or 0.0], dtype=torch.float64, device="cuda")
+        dist.all_reduce(te, op=dist.ReduceOp.SUM)
+        e2e = float(te[0])
+    h2d, d2h = batched_h2d_d2h(insts)
+    if rank != 0:
+        return None
+    chosen = r["chosen"]
+    peak, peak_kind = load_peaks()
+    bytes_per_step = r["cand_k"] * (4 + 4 + 1)
+    achieved = bytes_per_step * ant_steps_s / 1e9
+    line = {
+        "metric": "instances/s", "value": value, "unit": "instances/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None,
+        "dtype": "int32 weights + u8 pheromone (f64 route costs)", "data": "synthetic",
+        "config": {"workload": BATCHED["name"], "instances": BATCHED["count"],
+                   "step": "one solve of the whole batch (one persistent launch)",
+                   "tuning": {"cand_k": r["cand_k"], "lanes_per_ant": chosen[0],
+                              "ants_per_block": chosen[1],
+                              "order": "largest first" if chosen[2] else "as given"},
+                   "autotune_cand_k": r["per_k"],
+                   "autotune_trial_ms": [round(float(x), 3) for x in r["trials"]],
+                   "l2": "flushed between timed steps (256 MiB write outside the events)",
+                   "parallelism": f"instances split over {world} GPUs" if world > 1 else "1 GPU"},
+        "ant_steps_per_s": ant_steps_s,
+        "wall_s": r["wall"], "gpu_launches": args.steps,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "kernel": "k_batch_solve",
+                     "peak_kind": peak_kind, "bytes_per_ant_step": bytes_per_step},
+        "e2e": {"value": e2e, "unit": "instances/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "step": "set-up of the batch through the C ABI, one solve, download of "
+                        "every cost and best route"},
+        "looped_single_instance": r["looped"],
+        "clocks": r["clk"],
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline_batched(insts)
+        except Exception as exc:
+            line["cpu_baseline"] = {"error": str(exc)[:200]}
     return line
 
 
@@ -804,50 +844,63 @@ LEARNED = dict(train=4096, heldout=256, elite_ants=64, elite_k=16, elite_epochs=
 TRAIN_FLOPS_PER_EDGE = 2 * (8 * 64 + 64 * 64 + 64) + 2 * (64 * 64 + 64 * 64 + 8 * 64 + 64)
 
 
-def run_learned(args, rank, world, local, torch, dist, _native):
-    """Time-to-cost of the learned prior against plain eta on held-out
-    instances (one GPU; the whole pipeline -- elite routes by the plain
-    batched solver, training set, tensor-core training, gamma chosen on 8
-    validation instances, evaluation -- runs inside this call)."""
+def learned_measure(local, torch, _native, ntrain, nheld, nval):
+    """The learned prior's whole pipeline on one GPU: elite routes of the
+    plain batched solver on `ntrain` training instances, the training set,
+    tensor-core training, gamma for the learned levels and the beta of a
+    control (the plain solver with a sharper hand-set eta^beta) each chosen
+    on `nval` validation instances by mean final cost relative to the plain
+    solver, then time-to-cost on `nheld` held-out n=1000 instances."""
     from vehicleroutingproblem_b200 import prior as PR
-    if rank != 0:
-        return None
     L = LEARNED
-    ntrain = args.prior_train or L["train"]
-    nheld = args.prior_heldout or L["heldout"]
     tr = I.prior_training_instances(ntrain)
     t0 = time.perf_counter()
     sols = PR.elite_solutions(tr, ants=L["elite_ants"], cand_k=L["elite_k"],
                               epochs=L["elite_epochs"])
     elite_s = time.perf_counter() - t0
     pr = _native.Prior(local, seed=1)
-    t0 = time.perf_counter()
-    count = pr.set_dataset(tr, [(s[0], s[1]) for s in sols], cand_k=L["cand_k"])
-    dataset_s = time.perf_counter() - t0
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    losses = pr.train(L["train_epochs"], batch=L["batch"], lr=L["lr"], seed=11)
-    train_s = time.perf_counter() - t0
-    # gamma for the learned levels, and the control's beta (the plain solver
-    # with a sharper hand-set eta^beta), each chosen on 8 validation
-    # instances by the mean final cost relative to the plain solver.
-    val = [I.uniform_instance(1000, 8, 60000 + i) for i in range(L["validation"])]
-    base = PR.final_costs(val, L["epochs"], ants=L["ants"], cand_k=L["cand_k"])
-    scores = {g: float(np.mean(PR.final_costs(val, L["epochs"], pr, g, ants=L["ants"],
-                                              cand_k=L["cand_k"]) / base))
-              for g in L["gammas"]}
-    gamma = min(scores, key=lambda g: scores[g])
-    ctrl = {b: float(np.mean(PR.final_costs(val, L["epochs"], beta=b, ants=L["ants"],
-                                            cand_k=L["cand_k"]) / base))
-            for b in L["control_betas"]}
-    beta_c = min(ctrl, key=lambda b: ctrl[b])
-    held = I.prior_heldout_instances(nheld)
-    t0 = time.perf_counter()
-    res = PR.time_to_cost(held, pr, gamma=gamma, epochs=L["epochs"], ants=L["ants"],
-                          cand_k=L["cand_k"], control_beta=beta_c)
-    eval_s = time.perf_counter() - t0
-    rows = res.pop("rows")
+    try:
+        t0 = time.perf_counter()
+        count = pr.set_dataset(tr, [(x[0], x[1]) for x in sols], cand_k=L["cand_k"])
+        dataset_s = time.perf_counter() - t0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        losses = pr.train(L["train_epochs"], batch=L["batch"], lr=L["lr"], seed=11)
+        train_s = time.perf_counter() - t0
+        val = [I.uniform_instance(1000, 8, 60000 + i) for i in range(nval)]
+        base = PR.final_costs(val, L["epochs"], ants=L["ants"], cand_k=L["cand_k"])
+        scores = {g: float(np.mean(PR.final_costs(val, L["epochs"], pr, g, ants=L["ants"],
+                                                  cand_k=L["cand_k"]) / base))
+                  for g in L["gammas"]}
+        gamma = min(scores, key=lambda g: scores[g])
+        ctrl = {b: float(np.mean(PR.final_costs(val, L["epochs"], beta=b, ants=L["ants"],
+                                                cand_k=L["cand_k"]) / base))
+                for b in L["control_betas"]}
+        beta_c = min(ctrl, key=lambda b: ctrl[b])
+        held = I.prior_heldout_instances(nheld)
+        t0 = time.perf_counter()
+        res = PR.time_to_cost(held, pr, gamma=gamma, epochs=L["epochs"], ants=L["ants"],
+                              cand_k=L["cand_k"], control_beta=beta_c)
+        eval_s = time.perf_counter() - t0
+    finally:
+        pr.close()
     flops = TRAIN_FLOPS_PER_EDGE * 32.0 * count * L["train_epochs"]
+    return {"res": res, "gamma": gamma, "scores": scores, "beta_c": beta_c, "ctrl": ctrl,
+            "count": count, "losses": losses, "elite_s": elite_s, "dataset_s": dataset_s,
+            "train_s": train_s, "eval_s": eval_s, "flops": flops}
+
+
+def run_learned(args, rank, world, local, torch, dist, _native):
+    """Time-to-cost of the learned prior against plain eta on held-out
+    instances (one GPU; the whole pipeline runs inside this call)."""
+    if rank != 0:
+        return None
+    L = LEARNED
+    ntrain = args.prior_train or L["train"]
+    nheld = args.prior_heldout or L["heldout"]
+    r = learned_measure(local, torch, _native, ntrain, nheld, L["validation"])
+    res = r["res"]
+    rows = res.pop("rows")
     peak, peak_kind = None, "fallback"
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -855,7 +908,7 @@ def run_learned(args, rank, world, local, torch, dist, _native):
         peak_kind = "measured"
     except Exception:
         peak = 1590.0
-    achieved = flops / train_s / 1e12
+    achieved = r["flops"] / r["train_s"] / 1e12
     line = {
         "metric": "time-to-cost ratio (learned / plain eta)", "value": res["time_ratio_of_sums"],
         "unit": "ratio", "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": False,
@@ -863,23 +916,70 @@ def run_learned(args, rank, world, local, torch, dist, _native):
         "dtype": "bf16 MLP (fp32 accumulate) + int32 weights + u8 pheromone",
         "data": "synthetic",
         "config": {"workload": L["name"], "train_instances": ntrain, "heldout": nheld,
-                   "gamma": gamma, "gamma_validation_final_cost": scores,
-                   "control_beta": beta_c, "control_validation_final_cost": ctrl},
+                   "gamma": r["gamma"], "gamma_validation_final_cost": r["scores"],
+                   "control_beta": r["beta_c"], "control_validation_final_cost": r["ctrl"]},
         "time_to_cost": res,
-        "training": {"examples": count, "epochs": L["train_epochs"], "batch": L["batch"],
-                     "lr": L["lr"], "loss_first_last": [float(losses[0]), float(losses[-1])],
-                     "elite_s": elite_s, "dataset_s": dataset_s, "train_s": train_s,
-                     "examples_per_s": count * L["train_epochs"] / train_s},
+        "training": {"examples": r["count"], "epochs": L["train_epochs"], "batch": L["batch"],
+                     "lr": L["lr"],
+                     "loss_first_last": [float(r["losses"][0]), float(r["losses"][-1])],
+                     "elite_s": r["elite_s"], "dataset_s": r["dataset_s"], "train_s": r["train_s"],
+                     "examples_per_s": r["count"] * L["train_epochs"] / r["train_s"]},
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                      "kernel": "k_prior_mlp<train> with reduce, Adam and the per-epoch "
                                "shuffle upload (host-timed)",
                      "flops_per_edge": TRAIN_FLOPS_PER_EDGE},
-        "eval_s": eval_s,
+        "eval_s": r["eval_s"],
         "per_instance_sample": rows[:4],
     }
-    pr.close()
     return line
+
+
+def default_extras(local, torch, _native):
+    """The other two figures of the headline metric, on bounded samples so
+    that the default run stays within a few minutes: instances/s of the
+    batched form (the full 512-instance batch) against looping the plain
+    single-instance solver, and the learned prior's time-to-cost against
+    plain eta on a small held-out set, with the tuned-beta control."""
+    out = {}
+    insts = I.batched_instances(BATCHED["count"], BATCHED["seed0"])
+    try:
+        r = batched_measure(torch, local, _native, insts, BATCHED["seed0"], steps=3, warmup=1,
+                            e2e_steps=2, looped_sample=8)
+        value = r["count"] * 3 / (r["dev_ms"] / 1e3)
+        looped = r["looped"]
+        out["batched"] = {
+            "metric": "instances/s", "value": value, "unit": "instances/s",
+            "workload": BATCHED["name"], "steps": 3, "warmup": 1,
+            "ms_per_step": r["dev_ms"] / 3, "e2e": r["e2e"],
+            "tuning": {"cand_k": r["cand_k"], "lanes_per_ant": r["chosen"][0],
+                       "ants_per_block": r["chosen"][1],
+                       "order": "largest first" if r["chosen"][2] else "as given"},
+            "autotune_cand_k": r["per_k"],
+            "looped_single_instance": looped,
+            "vs_looped": value / looped["value"] if looped else None,
+            "mean_final_cost": r["mean_cost"], "clocks": r["clk"]}
+    except Exception as exc:  # reported, not fatal
+        out["batched"] = {"error": str(exc)[:300]}
+    try:
+        L = LEARNED
+        ntrain, nheld, nval = 512, 8, 4
+        r = learned_measure(local, torch, _native, ntrain, nheld, nval)
+        res = r["res"]
+        res.pop("rows")
+        out["learned_time_to_cost"] = {
+            "metric": "time-to-cost ratio (learned / plain eta)",
+            "value": res["time_ratio_of_sums"], "unit": "ratio", "higher_is_better": False,
+            "workload": (f"learned prior: {ntrain} training instances n~U[200,1000], {nheld} "
+                         f"held-out n=1000 K=8 (seeds 50000-{50000 + nheld - 1}), {nval} "
+                         f"validation, 256 ants 32-NN, {L['epochs']} epochs, target = plain "
+                         "final cost +0.5%"),
+            "gamma": r["gamma"], "control_beta": r["beta_c"], "time_to_cost": res,
+            "train_s": r["train_s"], "pipeline_s": r["elite_s"] + r["dataset_s"] +
+            r["train_s"] + r["eval_s"]}
+    except Exception as exc:  # reported, not fatal
+        out["learned_time_to_cost"] = {"error": str(exc)[:300]}
+    return out
 
 
 def main():
@@ -897,6 +997,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--looped-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="n1000: skip the batched and learned-prior figures added to the line")
     ap.add_argument("--no-large-update", action="store_true",
                     help="skip the n=16000 pheromone-sweep roofline of small workloads")
     ap.add_argument("--no-cli", dest="cli", action="store_false",

@@ -314,7 +314,29 @@ ACO_API int aco_b200_batch_get_tuning(aco_b200_batch *batch, aco_b200_batch_tuni
 ACO_API int aco_b200_batch_autotune(aco_b200_batch *batch, int trial_epochs,
                                     aco_b200_batch_tuning *chosen, float *trial_ms,
                                     int max_trials, int *n_trials);
-/* One launch solving every instance; _enqueue does not synchronise. */
+/* Rebuilds every instance's candidate lists and plain eta levels with
+ * length k (1 <= k <= 32, k <= every n; the lists are the first k of the
+ * nearest-neighbour order, as aco_b200_setup builds them).  A launch shape
+ * that cannot hold k (16 lanes per ant with k > 16) becomes the default
+ * {32, 16, 1}.  Learned levels applied before are replaced. */
+ACO_API int aco_b200_batch_set_cand_k(aco_b200_batch *batch, int k);
+ACO_API int aco_b200_batch_get_cand_k(aco_b200_batch *batch, int *k);
+/* Chooses the candidate-list length, then the launch shape.  Stage 1 solves
+ * the whole batch once per length ks[0..nks) (nks <= 16) on the default
+ * shape and records its device time (k_solve_ms), the mean final cost over
+ * the instances every length solved (k_mean_cost) and the instances solved
+ * (k_feasible).  The length kept is the fastest among those that solve the
+ * most instances and whose mean cost is within quality_tol (a fraction) of
+ * the best such mean: a shorter list cannot win on speed at the price of
+ * quality.  Stage 2 is aco_b200_batch_autotune at that length.  Any output
+ * pointer may be NULL. */
+ACO_API int aco_b200_batch_autotune_k(aco_b200_batch *batch, int trial_epochs, const int *ks,
+                                      int nks, double quality_tol,
+                                      aco_b200_batch_tuning *chosen, int *chosen_k,
+                                      double *k_solve_ms, double *k_mean_cost, int *k_feasible,
+                                      float *trial_ms, int max_trials, int *n_trials);
+/* One launch solving every instance (run as a CUDA graph that is kept while
+ * the launch's arguments stay the same); _enqueue does not synchronise. */
 ACO_API int aco_b200_batch_solve(aco_b200_batch *batch);
 ACO_API int aco_b200_batch_enqueue(aco_b200_batch *batch);
 ACO_API int aco_b200_batch_synchronize(aco_b200_batch *batch);

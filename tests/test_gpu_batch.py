@@ -77,6 +77,43 @@ def test_autotune_keeps_results():
         assert plain(insts[i], 9 + i, 32, 16, 6)[2] == c1[i]
 
 
+@pytest.mark.parametrize("k", [20, 32, 12])
+def test_set_cand_k_equals_single_instance_solver(k):
+    """Candidate lists rebuilt in place with another length give what the
+    single-instance solver gives at that length."""
+    insts = I.batched_instances(10, seed0=31500)
+    with _native.Batch(0) as b:
+        b.setup(insts, ants=16, cand_k=16, seed=40, epochs=8)
+        b.set_cand_k(k)
+        assert b.cand_k() == k
+        if k > 16:
+            assert b.tuning()[0] == 32  # 16 lanes cannot hold the list
+        b.solve()
+        for i in (0, 3, 9):
+            rn, rl, rc, re = plain(insts[i], 40 + i, 16, k, 8)
+            nodes, lens, cost, ep = b.best(i)
+            assert cost == rc and np.array_equal(nodes, rn) and np.array_equal(lens, rl)
+
+
+def test_autotune_chooses_candidate_length():
+    insts = I.batched_instances(24, seed0=31000)
+    with _native.Batch(0) as b:
+        b.setup(insts, ants=32, cand_k=16, seed=9, epochs=6)
+        k, shape, per, ms = b.autotune_k(ks=(16, 20, 32), quality_tol=0.005, trial_epochs=2)
+        assert b.cand_k() == k and b.tuning() == shape
+        assert sorted(per) == [16, 20, 32] and all(v[0] > 0 for v in per.values())
+        most = max(v[2] for v in per.values())
+        best = min(v[1] for v in per.values() if v[2] == most)
+        allowed = [kk for kk, v in per.items() if v[2] == most and v[1] <= best * 1.005]
+        assert k == min(allowed, key=lambda kk: per[kk][0])
+        assert len(ms) >= 3
+        b.solve()
+        c1, e1, _ = b.costs()
+        assert np.all(e1 == 6)
+    for i in (0, 7, 23):
+        assert plain(insts[i], 9 + i, 32, k, 6)[2] == c1[i]
+
+
 def test_setup_reuse_and_get_all(reference_runs):
     """One batch object solving a stream of batches: a smaller batch reuses
     the device buffers, a larger one reallocates them; every solve equals a

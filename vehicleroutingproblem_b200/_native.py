@@ -36,6 +36,7 @@ EXPORTED = [
     "aco_b200_batch_create", "aco_b200_batch_destroy", "aco_b200_batch_setup",
     "aco_b200_batch_set_stream",
     "aco_b200_batch_set_tuning", "aco_b200_batch_get_tuning", "aco_b200_batch_autotune",
+    "aco_b200_batch_set_cand_k", "aco_b200_batch_get_cand_k", "aco_b200_batch_autotune_k",
     "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
     "aco_b200_batch_get", "aco_b200_batch_get_costs", "aco_b200_batch_get_all",
     "aco_b200_shard_packet_ints", "aco_b200_shard_construct", "aco_b200_shard_update",
@@ -132,6 +133,9 @@ def load():
         "aco_b200_batch_setup": [vp, vp], "aco_b200_batch_set_tuning": [vp, vp],
         "aco_b200_batch_get_tuning": [vp, vp],
         "aco_b200_batch_autotune": [vp, i32, vp, vp, i32, vp],
+        "aco_b200_batch_set_cand_k": [vp, i32], "aco_b200_batch_get_cand_k": [vp, vp],
+        "aco_b200_batch_autotune_k": [vp, i32, vp, i32, C.c_double, vp, vp, vp, vp, vp, vp,
+                                      i32, vp],
         "aco_b200_batch_solve": [vp], "aco_b200_batch_enqueue": [vp],
         "aco_b200_batch_synchronize": [vp],
         "aco_b200_batch_get": [vp, i32, vp, vp, vp, vp],
@@ -601,6 +605,33 @@ class Batch:
         _check(self._lib.aco_b200_batch_autotune(self._h, trial_epochs, C.byref(t), _p(ms), 16,
                                                  C.byref(nt)), "aco_b200_batch_autotune")
         return t.as_tuple(), ms[: nt.value].copy()
+
+    def set_cand_k(self, k: int) -> None:
+        _check(self._lib.aco_b200_batch_set_cand_k(self._h, k), "aco_b200_batch_set_cand_k")
+
+    def cand_k(self) -> int:
+        k = C.c_int()
+        _check(self._lib.aco_b200_batch_get_cand_k(self._h, C.byref(k)),
+               "aco_b200_batch_get_cand_k")
+        return k.value
+
+    def autotune_k(self, ks=(16, 20, 32), quality_tol=0.005, trial_epochs=3):
+        """Candidate-list length, then launch shape (aco_b200_batch_autotune_k):
+        returns (k, shape, per-length {k: (solve ms, mean cost, solved)},
+        shape trial ms)."""
+        kk = np.array(ks, np.int32)
+        t = BatchTuning()
+        ck = C.c_int()
+        kms = np.zeros(len(ks), np.float64)
+        kcost = np.zeros(len(ks), np.float64)
+        kfeas = np.zeros(len(ks), np.int32)
+        ms = np.zeros(16, np.float32)
+        nt = C.c_int()
+        _check(self._lib.aco_b200_batch_autotune_k(
+            self._h, trial_epochs, _p(kk), len(ks), quality_tol, C.byref(t), C.byref(ck),
+            _p(kms), _p(kcost), _p(kfeas), _p(ms), 16, C.byref(nt)), "aco_b200_batch_autotune_k")
+        per = {int(k): (float(kms[i]), float(kcost[i]), int(kfeas[i])) for i, k in enumerate(ks)}
+        return ck.value, t.as_tuple(), per, ms[: nt.value].copy()
 
     def solve(self):
         _check(self._lib.aco_b200_batch_solve(self._h), "aco_b200_batch_solve")

@@ -637,11 +637,21 @@ struct aco_b200_batch {
   size_t arena_cap = 0, arena_used = 0;
   bool sizing = false;
   aco_b200_batch_tuning tuning = {32, 16, 1};
+  // The solve (queue reset + persistent launch) as a CUDA graph, kept while
+  // the launch's arguments are unchanged.
+  cudaGraphExec_t graph = nullptr;
+  std::vector<unsigned char> graph_key;
   const float *d_thr = nullptr;  // eta thresholds (plain levels)
   const long long *d_seg_off = nullptr;  // first row of every instance
   const int *d_seg_n = nullptr;          // customers of every instance
   long long rows = 0;                    // sum of n + 1
+  void drop_graph() {
+    if (graph) cudaGraphExecDestroy(graph);
+    graph = nullptr;
+    graph_key.clear();
+  }
   void free_all() {
+    drop_graph();
     if (arena) cudaFree(arena);
     arena = nullptr;
     arena_cap = arena_used = 0;
@@ -712,6 +722,7 @@ int aco_b200_batch_destroy(aco_b200_batch *b) {
 int aco_b200_batch_set_stream(aco_b200_batch *b, void *cuda_stream) {
   if (!b) return ACO_ERR_INVALID_INPUT;
   cudaSetDevice(b->device);
+  b->drop_graph();
   if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
   if (cuda_stream) {
     b->stream = (cudaStream_t)cuda_stream;
@@ -856,8 +867,10 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
     b->carve(&d_order, count);
     b->carve(&d_coords, node);
     b->carve(&d_dem, node);
-    b->carve(&d_cand, node * k);
-    b->carve(&d_lvl, node * k);
+    // Candidate tables sized for the longest list, so that
+    // aco_b200_batch_set_cand_k can rebuild them with any length in place.
+    b->carve(&d_cand, node * kMaxCand);
+    b->carve(&d_lvl, node * kMaxCand);
     b->carve(&d_A, 256);
     b->carve(&d_lut, 256);
     b->carve(&d_thr, kThresholds);
@@ -963,11 +976,44 @@ int aco_b200_batch_enqueue(aco_b200_batch *b) {
   if (per_sm < 1) return ACO_ERR_INVALID_INPUT;
   int grid = per_sm * b->num_sms;
   if (grid > b->count) grid = b->count;
-  BTRY(cudaMemsetAsync(b->args.queue, 0, sizeof(unsigned int), b->stream));
-  cudaError_t e = (t.lanes_per_ant == 16)
-                      ? launch_batch_lanes<16>(b->args, ly, grid, threads, t.ants_per_block, v, b->stream)
-                      : launch_batch_lanes<32>(b->args, ly, grid, threads, t.ants_per_block, v, b->stream);
-  BTRY(e);
+  auto record = [&](cudaStream_t s) -> cudaError_t {
+    cudaError_t e = cudaMemsetAsync(b->args.queue, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    return (t.lanes_per_ant == 16)
+               ? launch_batch_lanes<16>(b->args, ly, grid, threads, t.ants_per_block, v, s)
+               : launch_batch_lanes<32>(b->args, ly, grid, threads, t.ants_per_block, v, s);
+  };
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  BTRY(cudaStreamIsCapturing(b->stream, &cap));
+  if (cap != cudaStreamCaptureStatusNone) {
+    // The caller is capturing this stream into a graph of its own: record
+    // the solve there.
+    BTRY(record(b->stream));
+    return ACO_OK;
+  }
+  // The key: every argument of the two graph nodes.
+  std::vector<unsigned char> key(sizeof(BatchArgs) + sizeof(BatchSmem) + 4 * sizeof(int));
+  const int shape[4] = {grid, threads, t.ants_per_block, v * 64 + t.lanes_per_ant};
+  memcpy(key.data(), &b->args, sizeof(BatchArgs));
+  memcpy(key.data() + sizeof(BatchArgs), &ly, sizeof(BatchSmem));
+  memcpy(key.data() + sizeof(BatchArgs) + sizeof(BatchSmem), shape, sizeof(shape));
+  if (!b->graph || key != b->graph_key) {
+    b->drop_graph();
+    cudaGraph_t g = nullptr;
+    BTRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t err = record(b->stream);
+    const cudaError_t end = cudaStreamEndCapture(b->stream, &g);
+    if (err != cudaSuccess || end != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      BTRY(err != cudaSuccess ? err : end);
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) b->graph = nullptr;
+    BTRY(ie);
+    b->graph_key = key;
+  }
+  BTRY(cudaGraphLaunch(b->graph, b->stream));
   return ACO_OK;
 }
 
@@ -1021,6 +1067,119 @@ int aco_b200_batch_autotune(aco_b200_batch *b, int trial_epochs, aco_b200_batch_
   int rc = aco_b200_batch_set_tuning(b, &best);
   if (chosen) *chosen = best;
   return rc;
+}
+
+int aco_b200_batch_set_cand_k(aco_b200_batch *b, int k) {
+  if (!b || !b->ready || k < 1 || k > kMaxCand) return ACO_ERR_INVALID_INPUT;
+  for (const BatchInst &I : b->inst)
+    if (I.n < k) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(b->device);
+  BatchArgs &a = b->args;
+  BTRY(launch_knn_levels_multi(a.coords, b->d_seg_off, b->d_seg_n, b->count, b->rows, k,
+                               b->d_thr, kThresholds, const_cast<uint16_t *>(a.cand),
+                               const_cast<uint16_t *>(a.lvl), b->stream));
+  b->k = k;
+  a.k = k;
+  // The launch shape must hold the new list: keep it when it does, else the
+  // default shape (32 lanes per ant).
+  aco_b200_batch_tuning t = b->tuning;
+  if (aco_b200_batch_set_tuning(b, &t) != ACO_OK) {
+    t = aco_b200_batch_tuning{32, 16, 1};
+    const int rc = aco_b200_batch_set_tuning(b, &t);
+    if (rc) return rc;
+  }
+  BTRY(cudaStreamSynchronize(b->stream));
+  return ACO_OK;
+}
+
+int aco_b200_batch_get_cand_k(aco_b200_batch *b, int *k) {
+  if (!b || !b->ready || !k) return ACO_ERR_INVALID_INPUT;
+  *k = b->k;
+  return ACO_OK;
+}
+
+int aco_b200_batch_autotune_k(aco_b200_batch *b, int trial_epochs, const int *ks, int nks,
+                              double quality_tol, aco_b200_batch_tuning *chosen, int *chosen_k,
+                              double *k_solve_ms, double *k_mean_cost, int *k_feasible,
+                              float *trial_ms, int max_trials, int *n_trials) {
+  if (!b || !b->ready || !ks || nks < 1 || nks > 16 || !(quality_tol >= 0.0))
+    return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(b->device);
+  const int count = b->count;
+  std::vector<std::vector<double>> costs(nks);
+  std::vector<double> ms(nks, -1.0);
+  std::vector<int> valid(nks, 0);
+  cudaEvent_t e0, e1;
+  BTRY(cudaEventCreate(&e0));
+  BTRY(cudaEventCreate(&e1));
+  // Stage 1: one whole solve per candidate-list length, on the default
+  // launch shape (the shape does not change results, the length does).
+  for (int i = 0; i < nks; ++i) {
+    if (aco_b200_batch_set_cand_k(b, ks[i]) != ACO_OK) continue;
+    aco_b200_batch_tuning t = {32, 16, 1};
+    if (aco_b200_batch_set_tuning(b, &t) != ACO_OK) continue;
+    cudaEventRecord(e0, b->stream);
+    const int rc = aco_b200_batch_enqueue(b);
+    cudaEventRecord(e1, b->stream);
+    float t_ms = -1.f;
+    if (rc != ACO_OK || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&t_ms, e0, e1) != cudaSuccess)
+      continue;
+    costs[i].resize(count);
+    if (aco_b200_batch_get_costs(b, costs[i].data(), nullptr, nullptr) != ACO_OK) continue;
+    ms[i] = t_ms;
+    valid[i] = 1;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // Quality: the mean final cost over the instances every length solved;
+  // a length that leaves more instances without a solution is worse.
+  std::vector<int> infeasible(nks, 0);
+  std::vector<char> common(count, 1);
+  for (int i = 0; i < nks; ++i) {
+    if (!valid[i]) continue;
+    for (int j = 0; j < count; ++j) {
+      if (costs[i][j] >= DBL_MAX) {
+        infeasible[i] += 1;
+        common[j] = 0;
+      }
+    }
+  }
+  int min_inf = count + 1;
+  for (int i = 0; i < nks; ++i)
+    if (valid[i] && infeasible[i] < min_inf) min_inf = infeasible[i];
+  std::vector<double> mean(nks, DBL_MAX);
+  double best_mean = DBL_MAX;
+  for (int i = 0; i < nks; ++i) {
+    if (!valid[i]) continue;
+    double sum = 0.0;
+    int cnt = 0;
+    for (int j = 0; j < count; ++j)
+      if (common[j]) {
+        sum += costs[i][j];
+        ++cnt;
+      }
+    mean[i] = cnt ? sum / cnt : DBL_MAX;
+    if (infeasible[i] == min_inf && mean[i] < best_mean) best_mean = mean[i];
+  }
+  // The fastest length within quality_tol of the best quality.
+  int pick = -1;
+  for (int i = 0; i < nks; ++i) {
+    if (!valid[i] || infeasible[i] != min_inf) continue;
+    if (mean[i] > best_mean * (1.0 + quality_tol)) continue;
+    if (pick < 0 || ms[i] < ms[pick]) pick = i;
+  }
+  for (int i = 0; i < nks; ++i) {
+    if (k_solve_ms) k_solve_ms[i] = ms[i];
+    if (k_mean_cost) k_mean_cost[i] = valid[i] ? mean[i] : -1.0;
+    if (k_feasible) k_feasible[i] = valid[i] ? count - infeasible[i] : -1;
+  }
+  if (pick < 0) return ACO_ERR_INVALID_INPUT;
+  int rc = aco_b200_batch_set_cand_k(b, ks[pick]);
+  if (rc) return rc;
+  if (chosen_k) *chosen_k = ks[pick];
+  // Stage 2: the launch shape for that length.
+  return aco_b200_batch_autotune(b, trial_epochs, chosen, trial_ms, max_trials, n_trials);
 }
 
 int aco_b200_batch_get(aco_b200_batch *b, int instance, int *nodes, int *lens, double *cost,

@@ -144,6 +144,10 @@ ACO_API int aco_b200_get_plan(aco_b200_ctx *ctx, int out[4]);
 ACO_API int aco_b200_get_tau(aco_b200_ctx *ctx, uint8_t *tau);       /* (n+1)^2 */
 ACO_API int aco_b200_set_tau(aco_b200_ctx *ctx, const uint8_t *tau); /* (n+1)^2 */
 ACO_API int aco_b200_get_candidates(aco_b200_ctx *ctx, int *cand, uint16_t *levels);
+/* Neighbours of ranks k+1 .. k+64 of every node, in the candidates' order
+ * ([(n+1) 64], 0 = empty slot): where the construction's nearest-customer
+ * fallback looks before it scans every node. */
+ACO_API int aco_b200_get_tier(aco_b200_ctx *ctx, uint16_t *tier);
 ACO_API int aco_b200_get_tables(aco_b200_ctx *ctx, int32_t *A, uint32_t *lut,
                         float *thresholds, int n_thresholds);
 /* Weights recomputed from the current pheromone ((n+1) k values). */

@@ -102,6 +102,18 @@ def test_candidates_levels_tables(oracle_mod, name):
         assert np.array_equal(lvl, O.levels(inst.x, inst.y, ocand, kk, othr))
 
 
+@pytest.mark.parametrize("name", ["smoke", "small_c1", "u300_demand", "n1000_c2", "c2000_demand"])
+def test_fallback_tier_lists(oracle_mod, name):
+    """The fallback's neighbour lists: ranks k+1 .. k+64 of the oracle's
+    nearest-neighbour order (0 where fewer customers exist)."""
+    factory, k, m = CASES[name]
+    inst = factory()
+    with make_ctx(inst, k, 8) as ctx:
+        kk = ctx.k
+        full = oracle_mod.knn(inst.x, inst.y, kk + 64).reshape(inst.n + 1, kk + 64)
+        assert np.array_equal(ctx.tier().reshape(inst.n + 1, 64), full[:, kk:].astype(np.uint16))
+
+
 @pytest.mark.parametrize("name", ["u200_unit", "u300_demand", "n1000_c2"])
 @pytest.mark.parametrize("mode", ["random", "mostly_init"])
 def test_weights(oracle_mod, name, mode):

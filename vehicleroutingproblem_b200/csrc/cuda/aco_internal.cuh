@@ -119,7 +119,13 @@ struct InstanceView {
   const int *demand;       // [n+1]
   const uint16_t *cand;    // [(n+1) k]
   const uint16_t *lvl;     // [(n+1) k]
+  // Neighbours of ranks k+1 .. k+64 of every node in the candidates' order
+  // ([(n+1) kTierLen], 0 = none), or null: the nearest-customer fallback
+  // looks there before it scans every node.
+  const uint16_t *tier;
 };
+
+constexpr int kTierLen = 64;
 
 struct AntBuffers {
   int *routes;             // [m][n + 2K] compact routes
@@ -159,6 +165,7 @@ struct PheromoneView {
 cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
                               const float *thr, int J, uint16_t *cand,
                               uint16_t *lvl, cudaStream_t s);
+cudaError_t launch_knn_tier(const float2 *coords, int n, int k, uint16_t *tier, cudaStream_t s);
 // Candidate lists of `count` instances packed one after another: instance s
 // has seg_n[s] customers and starts at row seg_off[s] (device arrays).
 cudaError_t launch_knn_levels_multi(const float2 *coords, const long long *seg_off,
@@ -341,8 +348,11 @@ __device__ __forceinline__ void st_cg_u8(uint8_t *p, uint8_t v) {
 // t-th smallest (~0 when fewer than k exist).  Keys are unique, so the order
 // is total: ascending d^2, ties to the lower j, as the reference's insertion
 // with a strict '<' (aco_cuda_kernels.cu:187-201).
+// With `after` given (not ~0), the k smallest keys greater than it: the
+// next ranks of the same order.
 __device__ inline unsigned long long warp_knn(const float2 *coords, int n, int k,
-                                       int i, int lane) {
+                                       int i, int lane,
+                                       unsigned long long after = ~0ull) {
   const unsigned long long kNone = ~0ull;
   unsigned long long list = kNone;
   unsigned long long kth = kNone;
@@ -353,6 +363,7 @@ __device__ inline unsigned long long warp_knn(const float2 *coords, int n, int k
     if (j <= n && j != i) {
       float d2 = dist2f(pi, __ldg(coords + j));
       key = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)j;
+      if (after != kNone && key <= after) key = kNone;
     }
     unsigned m = __ballot_sync(kFull, key < kth);
     while (m) {

@@ -67,6 +67,38 @@ cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
   return cudaGetLastError();
 }
 
+// Neighbours of ranks k+1 .. k+64 of every node i (warp per node), the ranks
+// right after its k candidates: the 32 keys after the candidate list's last,
+// then the 32 after those, in the candidates' order (ascending d^2 bits, then
+// node).  0 marks an empty slot; an empty last slot means the candidates and
+// this row hold every other customer.
+__global__ void __launch_bounds__(256) k_knn_tier(const float2 *__restrict__ coords, int n,
+                                                  int k, uint16_t *__restrict__ tier) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const unsigned long long kNone = ~0ull;
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i <= n; i += warps) {
+    unsigned long long key = warp_knn(coords, n, k, i, lane);
+    int last_lane = k - 1;
+    uint16_t *row = tier + (size_t)i * kTierLen;
+#pragma unroll
+    for (int r = 0; r < kTierLen / 32; ++r) {
+      const unsigned long long last = __shfl_sync(kFull, key, last_lane);
+      key = (last == kNone) ? kNone : warp_knn(coords, n, 32, i, lane, last);
+      last_lane = 31;
+      row[32 * r + lane] = (uint16_t)(key == kNone ? 0u : (unsigned)(key & 0xffffffffu));
+    }
+  }
+}
+
+cudaError_t launch_knn_tier(const float2 *coords, int n, int k, uint16_t *tier, cudaStream_t s) {
+  if (k < 1 || k > kMaxCand) return cudaErrorInvalidValue;
+  int blocks = (n + 1 + 7) / 8;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_knn_tier<<<blocks, 256, 0, s>>>(coords, n, k, tier);
+  return cudaGetLastError();
+}
+
 // Candidate lists of many instances in one launch.  Instance s owns rows
 // [seg_off[s], seg_off[s] + seg_n[s] + 1) of the concatenated coordinates
 // (seg_off ascending); each warp finds its row's instance by binary search and
@@ -236,6 +268,7 @@ __device__ __forceinline__ void draw_refill(uint32_t *buf, uint32_t d,
 
 template <int L, bool UNIT>
 struct Tables {
+  const uint16_t *tier;  // global, or null
   const uint16_t *cand;
   const uint32_t *w;
   const uint8_t *rel;
@@ -357,6 +390,33 @@ __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
   const uint32_t mh = __reduce_min_sync(kFull, best_h);
   const uint32_t mn = __reduce_min_sync(kFull, best_h == mh ? best_n : 0xffffffffu);
   return (mh == 0xffffffffu) ? 0 : (int)mn;
+}
+
+// Nearest eligible customer of the fallback, when no candidate of row cur
+// has a weight (find_nearest_unvisited's rule, as nearest_unvisited): the
+// first eligible candidate (okm: the row's eligible candidates; they come
+// first in the order), else the first eligible node of the tier row (the
+// next 64 ranks of the same order), else the full scan; 0 when the
+// candidates and a complete tier row hold no eligible customer.
+template <int L, bool UNIT, int V>
+__device__ __forceinline__ int nearest_eligible(const Tables<L, UNIT> &tb, const Visited<V> &vis,
+                                                int cur, unsigned okm, int c, int room,
+                                                bool check_dem, int lane) {
+  if (okm) return __shfl_sync(kFull, c, __ffs(okm) - 1);
+  if (tb.tier) {
+    const uint16_t *row = tb.tier + (size_t)cur * kTierLen;
+    int node = 0;
+#pragma unroll
+    for (int r = 0; r < kTierLen / 32; ++r) {
+      node = (int)__ldg(row + 32 * r + lane);
+      bool ok = !vis.test(node);  // node 0 (empty slot) reads as visited
+      if (!UNIT && check_dem && ok) ok = tb.demand(node) <= room;
+      const unsigned m = __ballot_sync(kFull, ok);
+      if (m) return __shfl_sync(kFull, node, __ffs(m) - 1);
+    }
+    if (__shfl_sync(kFull, node, 31) == 0) return 0;  // every customer was listed
+  }
+  return nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), room, check_dem, lane);
 }
 
 struct ConstructArgs {
@@ -486,25 +546,29 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
     bool tight = !UNIT && 0 > tight_load;
     // Row of the current node; the next row's loads are issued as soon as the
     // next node is known, ahead of this step's bookkeeping.
-    int c = 0, dc = 0;
+    // cb: this lane's candidate's row offset, formed as soon as the row is
+    // loaded, so the selected lane's offset reaches the next row's loads by
+    // one shuffle, with no multiply on the chain.
+    int c = 0, dc = 0, cb = 0;
     uint32_t w = 0u;
     if (lane < k) {
       c = tb.cand[lane];
       w = tb.weight(lane);
     }
+    cb = c * k;
     if (!UNIT) dc = tb.demand(c);
     // Every demand is >= 1, so rem_dem > future >= 0 implies remaining > 0.
     const int limit = CREF ? 0 : future;
-    // One step to customer nx of demand dnx: the next row's loads first,
-    // then the bookkeeping.
-    auto take_step = [&](int nx, int dnx) {
-      const int base = nx * k;
+    // One step to customer nx (row offset base = nx k) of demand dnx: the
+    // next row's loads first, then the bookkeeping.
+    auto take_step = [&](int nx, int base, int dnx) {
       c = 0;
       w = 0u;
       if (lane < k) {
         c = tb.cand[base + lane];
         w = tb.weight(base + lane);
       }
+      cb = c * k;
       if (!UNIT) dc = tb.demand(c);
       route[pos] = nx;  // every lane stores the same value
       vis.set(nx, lane);
@@ -531,14 +595,19 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       // cum * 2^24 >= r * denom  <=>  cum >= ceil(r * denom / 2^24)
       const uint32_t thr =
           (uint32_t)(((unsigned long long)r_next * denom + 0xFFFFFFull) >> kDrawBits);
-      // Inclusive scan; lanes 0..7 hold their full prefix after three steps,
-      // and most draws land there, so the last two steps run only if needed.
-      uint32_t cum = wv;
+      // Sum of the 8 masked weights ending at this lane (lanes 0..7: the
+      // inclusive prefix, where most draws land): 7 independent shuffles of
+      // the weights and an add tree, the value three scan steps give with
+      // three dependent shuffles.  The last two scan steps run only if
+      // needed.
+      uint32_t u[8];
+      u[0] = wv;
 #pragma unroll
-      for (int o = 1; o < 8; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(kFull, cum, o);
-        if (lane >= o) cum += t;
+      for (int o = 1; o < 8; ++o) {
+        const uint32_t t = __shfl_up_sync(kFull, wv, o);
+        u[o] = lane >= o ? t : 0u;
       }
+      uint32_t cum = ((u[0] + u[1]) + (u[2] + u[3])) + ((u[4] + u[5]) + (u[6] + u[7]));
       unsigned msk = __ballot_sync(kFull, lane < 8 && wv != 0u && cum >= thr);
       if (msk == 0u) {
 #pragma unroll
@@ -552,14 +621,15 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
           // when it may; otherwise the nearest eligible customer, which
           // consumes no draw.
           if (CREF && may_close) break;
-          const int nx = nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), cap - load,
-                                                       tight, lane);
+          const int nx = nearest_eligible<L, UNIT, V>(tb, vis, cur, __ballot_sync(kFull, ok), c,
+                                                      cap - load, tight, lane);
           if (nx <= 0) break;
-          take_step(nx, tb.demand(nx));
+          take_step(nx, nx * k, tb.demand(nx));
           continue;
         }
       }
       const int src = __ffs(msk) - 1;  // msk != 0 here: denom > 0
+      const int nbase = __shfl_sync(kFull, cb, src);
       int next = __shfl_sync(kFull, c, src);
       int dn = UNIT ? 1 : __shfl_sync(kFull, dc, src);
       bool drawn = false;  // draws of this step already accounted
@@ -575,7 +645,7 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
         if (__dmul_rn((double)r2, __dadd_rn((double)denom, wd)) >= (double)denom * 16777216.0)
           break;
       }
-      take_step(next, dn);
+      take_step(next, nbase, dn);
       // A draw is consumed only by a roulette selection (denom > 0).
       if (!drawn) {
         d += 1u;
@@ -664,6 +734,7 @@ __global__ void __launch_bounds__(512, 1) k_construct(ConstructArgs a) {
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
 
   Tables<L, UNIT> tb;
+  tb.tier = iv.tier;
   if (L == kLayoutGlobal) {
     tb.cand = iv.cand;
     tb.w = a.et.w;

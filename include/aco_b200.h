@@ -383,7 +383,10 @@ ACO_API int aco_b200_batch_apply_prior(aco_b200_batch *batch, aco_b200_prior *pr
  * shares that array: calls whose kernels overlap on the GPU race, so issue
  * them on one stream or otherwise order them.  The first call on each
  * device looks up the array's device address (cudaGetSymbolAddress); make
- * that first call before capturing a stream into a CUDA graph.
+ * that first call before capturing a stream into a CUDA graph.  The address
+ * is kept for the life of the process: it does not survive a device reset
+ * (cudaDeviceReset, or the primary context destroyed and made again), after
+ * which this entry point must not be called in the same process.
  */
 ACO_API int aco_b200_evaporate_deposit_noalloc(uint8_t *d_tau, int n, int K,
                                                const int *d_iter_nodes,

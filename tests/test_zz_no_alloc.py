@@ -30,14 +30,26 @@ def _entry():
     return f
 
 
+def _at_capacity():
+    """4096 routes, the most the fixed scratch holds: 4500 unit-demand
+    customers, at most 2 per vehicle, so the early vehicles stay empty and
+    the last route offset is the scratch's last word."""
+    base = I.uniform_instance(4500, 4096, 908).unit_twin()
+    return I.Instance("noalloc_cap", base.x, base.y, base.demand, 4096, 2), 4, 8
+
+
+@pytest.mark.parametrize("case", ["n300_K6", "K4096"])
 @pytest.mark.parametrize("with_global", [True, False])
-def test_no_alloc_matches_context_entry_point(with_global):
+def test_no_alloc_matches_context_entry_point(with_global, case):
     import torch
     noalloc = _entry()
-    inst = I.uniform_instance(300, 6, 907)
+    if case == "K4096":
+        inst, ants, k = _at_capacity()
+    else:
+        inst, ants, k = I.uniform_instance(300, 6, 907), 16, 20
     n, K = inst.n, inst.vehicles
     with _native.Context(0) as ctx:
-        ctx.setup_instance(inst, ants=16, cand_k=20, seed=11)
+        ctx.setup_instance(inst, ants=ants, cand_k=k, seed=11)
         tau0 = np.random.RandomState(5).randint(0, 256, size=(n + 1) ** 2).astype(np.uint8)
         ctx.set_tau(tau0)
         ctx.construct(0)

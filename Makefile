@@ -20,7 +20,7 @@ LIB := $(PKG)/libaco_b200.so
 CLI := aco_vrp_cuda.out
 
 CU_SRCS := $(CSRC)/cuda/aco_kernels.cu $(CSRC)/cuda/aco_solver.cu $(CSRC)/cuda/aco_compat.cu $(CSRC)/cuda/aco_prior.cu \
-           $(CSRC)/cuda/aco_noalloc.cu $(CSRC)/cuda/aco_batch.cu
+           $(CSRC)/cuda/aco_noalloc.cu $(CSRC)/cuda/aco_batch.cu $(CSRC)/cuda/aco_seq_update.cu
 C_SRCS := $(CSRC)/common/solution.c $(CSRC)/common/instance_parser.c \
           $(CSRC)/common/aco_config.c $(CSRC)/common/cli_common.c
 CU_OBJS := $(patsubst $(CSRC)/cuda/%.cu,$(BUILD)/%.o,$(CU_SRCS))

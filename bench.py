@@ -32,7 +32,9 @@ n=1000 instances (training set, training and evaluation inside the run).
 * roofline_update: the pheromone evaporation sweep, 2 (n+1)^2 bytes per
   launch over its mean event-timed duration, timed alone; where the
   workload's matrices fit in L2 (n1000, small, clustered2000) the line also
-  carries roofline_update_hbm, the same sweep on an n=16000 matrix pair.
+  carries roofline_update_hbm, the same sweep on an n=16000 matrix pair, and
+  roofline_seq_update_hbm, the sequential path's FP64 update on an n=16000
+  matrix (16 bytes per cell).
 * batched / learned_time_to_cost (default n1000 run only, --no-extras skips
   them): the other two figures of the headline metric -- instances/s of the
   batched form on the full 512-instance batch beside the single-instance
@@ -433,6 +435,52 @@ def update_roofline(ctx, n, launches, peak, peak_kind):
                                else None)}
 
 
+def seq_update_roofline(torch, ctx, n, K, launches, peak, peak_kind):
+    """Roofline of the sequential path's FP64 pheromone update
+    (aco_b200_seq_pheromone_update; the reference's evaporation, deposits,
+    MMAS clamp and reset loops, src/seq/aco_sequential.c:829-886) on an
+    (n+1)^2 FP64 matrix: 16 algorithmic bytes per cell (each cell read and
+    written once) over the mean CUDA-event time of one update, with the
+    stagnation reset on; the solutions are two ants of `ctx` (set up on the
+    same instance)."""
+    from vehicleroutingproblem_b200 import _native
+    L = _native.load()
+    ctx.construct(0)
+    nodes, lens, cost, _, _, _ = ctx.ants()
+    sol = [(torch.from_numpy(nodes[a][: lens[a].sum()].astype(np.int32)).cuda(),
+            torch.from_numpy(lens[a].astype(np.int32)).cuda(), float(cost[a])) for a in (0, 1)]
+    tau = torch.full(((n + 1) * (n + 1),), 0.01, dtype=torch.float64, device="cuda")
+    scratch = torch.zeros(L.aco_b200_seq_update_scratch_bytes(n), dtype=torch.uint8,
+                          device="cuda")
+    stream = torch.cuda.current_stream()
+    tmax = 1.0 / (0.9 * sol[1][2])
+
+    def call():
+        return L.aco_b200_seq_pheromone_update(
+            tau.data_ptr(), n, K, sol[0][0].data_ptr(), sol[0][1].data_ptr(), 0.3 / sol[0][2],
+            sol[1][0].data_ptr(), sol[1][1].data_ptr(), 0.7 / sol[1][2], 0.1, 0.05 * tmax, tmax,
+            1, 1.0, scratch.data_ptr(), stream.cuda_stream)
+
+    assert call() == 0  # warm-up
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(launches)]
+    for e0, e1 in evs:
+        e0.record(stream)
+        assert call() == 0
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in evs) / launches
+    nbytes = 16 * (n + 1) ** 2
+    achieved = nbytes / (ms / 1e3) / 1e9
+    del tau, scratch
+    return {"bound": "hbm", "kernel": "k_seq_sweep + k_seq_mark + k_seq_deposit",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": peak_kind, "n": n, "bytes_per_update": nbytes,
+            "us_per_update": ms * 1e3, "launches": launches, "traffic": None,
+            "note": ("FP64 matrix of the sequential path; the reference's loops make three "
+                     "passes over it (48 bytes per cell with the reset), this update one")}
+
+
 def timed_steps(torch, stream, steps, enqueue, flush):
     """Device ms of `steps` calls of enqueue(), each bracketed by events, the
     L2 flushed between steps outside the events."""
@@ -478,7 +526,7 @@ def run_single(args, rank, world, local, torch, dist, _native):
     kms = ctx.profile_epochs(32) / 32.0
     peak, peak_kind = load_peaks()
     roof_upd = update_roofline(ctx, n, 200 if n <= 4000 else 50, peak, peak_kind)
-    roof_upd_hbm = None
+    roof_upd_hbm = roof_seq_hbm = None
     if rank == 0 and (n + 1) ** 2 * 2 <= L2_BYTES and not args.no_large_update:
         # The matrix of this workload stays in L2; the same sweep on an
         # n=16000 matrix pair (512 MB) gives the HBM figure.
@@ -487,6 +535,8 @@ def run_single(args, rank, world, local, torch, dist, _native):
             cl.set_stream(stream.cuda_stream)
             cl.setup_instance(big, ants=32, cand_k=k, seed=5)
             roof_upd_hbm = update_roofline(cl, big.n, 50, peak, peak_kind)
+            roof_seq_hbm = seq_update_roofline(torch, cl, big.n, big.vehicles, 10, peak,
+                                               peak_kind)
     t = torch.tensor([dev_ms, float(steps_done)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
@@ -558,6 +608,8 @@ def run_single(args, rank, world, local, torch, dist, _native):
         }
         if roof_upd_hbm is not None:
             line["roofline_update_hbm"] = roof_upd_hbm
+        if roof_seq_hbm is not None:
+            line["roofline_seq_update_hbm"] = roof_seq_hbm
         if world == 1 and args.workload == "n1000" and not args.no_extras:
             line.update(default_extras(local, torch, _native))
         if world == 1 and not args.no_cpu_baseline:

@@ -397,6 +397,36 @@ ACO_API int aco_b200_evaporate_deposit_noalloc(uint8_t *d_tau, int n, int K,
                                                float dep_global, double rho,
                                                void *cuda_stream);
 
+/*
+ * The sequential path's FP64 pheromone update (src/seq/aco_sequential.c:
+ * 829-886, run there when an iteration best exists), bit-exact on a device
+ * matrix: tau[i][j] *= (1 - rho) for i != j; tau[u][v] += iter_deposit and
+ * tau[v][u] += iter_deposit over every arc of the iteration best, then the
+ * same with best_deposit over the global best (d_best_* NULL to skip, as
+ * the reference skips it while it has no best); every off-diagonal cell
+ * clamped to [tau_min, tau_max] (MMAS); then, when `reset` is nonzero (the
+ * reference's stagnation trigger), tau[i][j] = 0.5 tau[i][j] + 0.5 tau0 for
+ * i != j.  iter_deposit and best_deposit are the reference's
+ * (weight * Q) / cost values.
+ *
+ * d_tau: (n+1)^2 doubles, row-major, row stride n+1.  Solutions in compact
+ * form (K segments [0 c.. 0] back to back, K lengths), K <= 8192, device
+ * memory.  d_scratch: aco_b200_seq_update_scratch_bytes(n) bytes of device
+ * memory, zeroed by the caller before the first call; every call leaves it
+ * zeroed again.  The update runs on `cuda_stream` (NULL: the default
+ * stream) in three launches: one sweep of the matrix (evaporation, and
+ * clamp/reset of every cell no deposit touches) and two small kernels over
+ * the solutions' arcs.
+ */
+ACO_API size_t aco_b200_seq_update_scratch_bytes(int n);
+ACO_API int aco_b200_seq_pheromone_update(double *d_tau, int n, int K,
+                                          const int *d_iter_nodes, const int *d_iter_lens,
+                                          double iter_deposit, const int *d_best_nodes,
+                                          const int *d_best_lens, double best_deposit,
+                                          double rho, double tau_min, double tau_max,
+                                          int reset, double tau0, void *d_scratch,
+                                          void *cuda_stream);
+
 /* Library build information. */
 ACO_API const char *aco_b200_build_info(void);
 

@@ -270,3 +270,34 @@ def ref_cost(x, y, nodes, lens) -> float:
                                       _p(np.ascontiguousarray(y, np.float32)),
                                       _p(np.ascontiguousarray(nodes, np.int32)),
                                       _p(np.ascontiguousarray(lens, np.int32)))
+
+
+def seq_pheromone_update(tau, n, it_nodes, it_lens, d_it, gb_nodes, gb_lens, d_gb, rho,
+                         tau_min, tau_max, reset, tau0) -> np.ndarray:
+    """The sequential path's FP64 pheromone update (src/seq/aco_sequential.c:
+    829-886) on an (n+1)^2 row-major matrix: evaporation of every i != j by
+    (1 - rho); both directions of every arc of the iteration best, then of
+    the global best (gb_nodes None to skip), arc by arc in route order; the
+    MMAS clamp of every i != j; the 0.5 tau + 0.5 tau0 reset when `reset`.
+    numpy's float64 element-wise operations are single IEEE operations in
+    this order, as the reference's loops are."""
+    t = np.array(tau, dtype=np.float64).reshape(n + 1, n + 1).copy()
+    off = ~np.eye(n + 1, dtype=bool)
+    t[off] = t[off] * (1.0 - rho)
+    for nodes, lens, d in ((it_nodes, it_lens, d_it), (gb_nodes, gb_lens, d_gb)):
+        if nodes is None:
+            continue
+        nodes = np.asarray(nodes, np.int64)
+        e = 0
+        for ln in lens:
+            for q in range(int(ln) - 1):
+                u, v = nodes[e + q], nodes[e + q + 1]
+                t[u, v] += d
+                t[v, u] += d
+            e += int(ln)
+    x = t[off]
+    x = np.where(x < tau_min, tau_min, np.where(x > tau_max, tau_max, x))
+    if reset:
+        x = 0.5 * x + 0.5 * tau0
+    t[off] = x
+    return t.ravel()

@@ -239,3 +239,50 @@ def test_cuda_ref_depot_rule_serves_everyone(oracle_mod):
                                          5, 0, a)
         differs += int(not np.array_equal(lens, l0) or not np.array_equal(nodes, n0))
     assert differs > 0
+
+
+def _seq_update_loops(tau, n, solutions, rho, tau_min, tau_max, reset, tau0):
+    """The reference's update written as its scalar loops
+    (src/seq/aco_sequential.c:829-886), for small n."""
+    t = [list(map(float, tau[i * (n + 1):(i + 1) * (n + 1)])) for i in range(n + 1)]
+    for i in range(n + 1):
+        for j in range(n + 1):
+            if i != j:
+                t[i][j] *= (1.0 - rho)
+    for nodes, lens, d in solutions:
+        e = 0
+        for ln in lens:
+            for q in range(ln - 1):
+                u, v = int(nodes[e + q]), int(nodes[e + q + 1])
+                t[u][v] += d
+                t[v][u] += d
+            e += ln
+    for i in range(n + 1):
+        for j in range(n + 1):
+            if i == j:
+                continue
+            if t[i][j] < tau_min:
+                t[i][j] = tau_min
+            elif t[i][j] > tau_max:
+                t[i][j] = tau_max
+    if reset:
+        for i in range(n + 1):
+            for j in range(n + 1):
+                if i != j:
+                    t[i][j] = 0.5 * t[i][j] + 0.5 * tau0
+    return np.array(t, np.float64).ravel()
+
+
+@pytest.mark.parametrize("reset", [False, True])
+def test_seq_update_restatement_equals_scalar_loops(oracle_mod, reset):
+    n = 20
+    rs = np.random.RandomState(3)
+    tau = rs.uniform(0.001, 0.05, size=(n + 1) ** 2)
+    it = (np.array([0, 3, 7, 0, 0, 0, 1, 2, 4, 5, 6, 8, 9, 10, 0], np.int32),
+          np.array([4, 2, 9], np.int32), 0.013)
+    gb = (np.array([0, 7, 3, 1, 0, 0, 2, 4, 5, 0, 0, 6, 8, 9, 10, 0], np.int32),
+          np.array([5, 5, 6], np.int32), 0.021)
+    got = oracle_mod.seq_pheromone_update(tau, n, it[0], it[1], it[2], gb[0], gb[1], gb[2],
+                                          0.1, 0.004, 0.04, reset, 1.0)
+    ref = _seq_update_loops(tau, n, [it, gb], 0.1, 0.004, 0.04, reset, 1.0)
+    assert np.array_equal(got.view(np.uint64), ref.view(np.uint64))

@@ -33,6 +33,7 @@ EXPORTED = [
     "aco_b200_get_tables", "aco_b200_get_weights", "aco_b200_construct",
     "aco_b200_get_ants", "aco_b200_evaporate_deposit", "aco_b200_build_info",
     "aco_b200_profile_epochs", "aco_b200_profile_update", "aco_b200_evaporate_deposit_noalloc",
+    "aco_b200_seq_update_scratch_bytes", "aco_b200_seq_pheromone_update",
     "aco_b200_batch_create", "aco_b200_batch_destroy", "aco_b200_batch_setup",
     "aco_b200_batch_set_stream",
     "aco_b200_batch_set_tuning", "aco_b200_batch_get_tuning", "aco_b200_batch_autotune",
@@ -163,6 +164,12 @@ def load():
         fn = getattr(L, name)
         fn.argtypes = args
         fn.restype = i32
+    L.aco_b200_seq_update_scratch_bytes.argtypes = [i32]
+    L.aco_b200_seq_update_scratch_bytes.restype = C.c_size_t
+    f64 = C.c_double
+    L.aco_b200_seq_pheromone_update.argtypes = [vp, i32, i32, vp, vp, f64, vp, vp, f64, f64,
+                                                f64, f64, i32, f64, vp, vp]
+    L.aco_b200_seq_pheromone_update.restype = i32
     L.aco_b200_prior_num_examples.argtypes = [vp]
     L.aco_b200_prior_num_examples.restype = C.c_longlong
     L.aco_b200_build_info.restype = C.c_char_p

@@ -20,6 +20,9 @@ best mean final cost) and the launch shape; a step is one solve of the
 whole batch and the metric is instances/s.
 learned: the learned prior's time-to-cost against plain eta on 256 held-out
 n=1000 instances (training set, training and evaluation inside the run).
+costdist: not a throughput line -- the best cost over seeds at fixed epochs
+of this library's CLI (both depot rules) and the reference's own CUDA
+solver, same CLI contract, same GPU, unit-demand twin of n1000.
 
 * value: device time (CUDA events on the library's stream), L2 flushed by a
   256 MiB write between steps outside the events, all ranks' work over the
@@ -366,6 +369,79 @@ def cli_epoch_rate(binary, inst, ants, seconds=CLI_SECONDS, extra_env=None):
             "best_cost": float(cost[-1]) if cost else None,
             "instance": f"unit-demand twin n={n} K={K} capacity={twin.capacity}",
             "ants": ants, "timeout_s": seconds}
+
+
+def cli_trajectory(binary, twin, ants, seed, seconds, extra_env=None):
+    """Every progress line of one solver binary run with the reference CLI
+    contract on a unit-demand instance: [(epoch, elapsed s, best cost)]."""
+    import re
+    env = dict(os.environ, ACO_SOLVER_TIMEOUT_SECONDS=str(seconds),
+               ACO_SOLVER_STAGNATION_EPOCHS="0", ACO_SOLVER_PROGRESS_INTERVAL_SECONDS="0")
+    env.pop("ACO_SOLVER_FIXED_EPOCHS", None)
+    env.update(extra_env or {})
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, twin.name + ".vrp")
+        I.write_vrp(twin, path)
+        r = subprocess.run([binary, path, str(twin.vehicles), str(ants), str(seed)], env=env,
+                           capture_output=True, text=True, timeout=seconds + 300)
+    if r.returncode != 0:
+        raise RuntimeError(f"{os.path.basename(binary)} exit {r.returncode}: {r.stderr[-300:]}")
+    return [(int(e), float(t), float(c)) for e, t, c in re.findall(
+        r"epoca=(\d+) .*tempo_trascorso=([0-9.]+)s .*best_cost=([0-9.]+)", r.stdout)]
+
+
+def run_costdist(args):
+    """Cost-quality distribution over seeds of three solvers behind the same
+    CLI on the same GPU: this library's aco_vrp_cuda.out with the default
+    (sequential) rules and with ACO_CUDA_DEPOT_RULE=cuda_ref, and the
+    reference's own CUDA solver built from its sources for sm_100a
+    (src/cuda/aco_cuda.cu, aco_cuda_kernels.cu), on the unit-demand twin of
+    the n1000 workload.  Each run has the same wall-time limit; the best
+    cost is read at fixed epochs from the progress lines (printed at epoch
+    1, every 10th epoch and on each improvement)."""
+    twin = I.workload_n1000().unit_twin()
+    ants, secs = 256, args.costdist_seconds
+    marks = (10, 100, 300, 1000)
+    solvers = [("b200 default rule", OUR_CLI, {}),
+               ("b200 cuda_ref rule", OUR_CLI, {"ACO_CUDA_DEPOT_RULE": "cuda_ref"}),
+               ("reference CUDA solver", REF_CUDA_BIN, {})]
+    out = {}
+    for name, binary, env in solvers:
+        if not os.path.exists(binary):
+            out[name] = {"error": f"{binary} not built"}
+            continue
+        per_seed = []
+        for seed in range(1, args.costdist_seeds + 1):
+            tr = cli_trajectory(binary, twin, ants, seed, secs, env)
+            at = {}
+            for mk in marks:
+                seen = [c for e, _, c in tr if e <= mk]
+                at[mk] = seen[-1] if seen and tr[-1][0] >= mk else None
+            e_last, t_last, c_last = tr[-1]
+            per_seed.append({"seed": seed, "best_at": at, "final": c_last, "epochs": e_last,
+                             "epochs_per_s": e_last / t_last if t_last > 0 else None})
+
+        def stats(v):
+            v = np.array([x for x in v if x is not None], float)
+            if not len(v):
+                return None
+            return {"mean": float(v.mean()), "median": float(np.median(v)),
+                    "std": float(v.std(ddof=1)) if len(v) > 1 else 0.0,
+                    "min": float(v.min()), "max": float(v.max()), "runs": int(len(v))}
+        out[name] = {"best_at_epoch": {str(mk): stats([r["best_at"][mk] for r in per_seed])
+                                       for mk in marks},
+                     "final": stats([r["final"] for r in per_seed]),
+                     "epochs_per_s": stats([r["epochs_per_s"] for r in per_seed]),
+                     "per_seed": per_seed}
+    line = {"metric": "best cost over seeds at fixed epochs (same CLI, same GPU)",
+            "unit": "route cost (FP64)", "higher_is_better": False,
+            "config": {"instance": f"unit-demand twin of the n1000 workload: n={twin.n} "
+                                   f"K={twin.vehicles} capacity={twin.capacity}",
+                       "ants": ants, "seeds": args.costdist_seeds, "timeout_s": secs,
+                       "stagnation": "off"},
+            "solvers": out}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def run_reference_arm(args, rank, world):
@@ -1041,7 +1117,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=None)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="n1000",
-                    choices=sorted(WORKLOADS) + ["batched", "learned"])
+                    choices=sorted(WORKLOADS) + ["batched", "learned", "costdist"])
+    ap.add_argument("--costdist-seeds", type=int, default=12,
+                    help="costdist: seeds per solver")
+    ap.add_argument("--costdist-seconds", type=float, default=2.0,
+                    help="costdist: wall-time limit of each run")
     ap.add_argument("--prior-train", type=int, default=None,
                     help="learned: training instances (default 4096)")
     ap.add_argument("--prior-heldout", type=int, default=None,
@@ -1068,6 +1148,8 @@ def main():
         args.e2e_steps = 3 if batched else 8
     args.warmup = max(args.warmup, 3)
     rank, world, local = dist_env()
+    if args.workload == "costdist":
+        return run_costdist(args) if rank == 0 else 0
 
     if args.impl == "reference":
         if args.workload == "learned":

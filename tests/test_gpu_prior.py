@@ -5,6 +5,7 @@ and their use by the exact construction path."""
 import numpy as np
 import pytest
 
+from vehicleroutingproblem_b200 import _native
 from vehicleroutingproblem_b200 import instances as I
 
 pytestmark = pytest.mark.gpu
@@ -235,6 +236,32 @@ def test_time_to_cost_pipeline(dataset):
     row = res["rows"][0]
     assert res["instances"] == 1 and 1 <= row["plain_epochs"] <= 30
     assert row["plain_s"] > 0 and row["learned_s"] > 0 and row["prior_s"] > 0
+
+
+def test_learned_prior_gains_over_plain_eta():
+    """What the trained network gains over the method without it: on
+    held-out n=1000 instances the learned levels reach the plain solver's
+    final cost (+0.5 %, FP64) in under half its time.  The control -- the
+    plain solver with a hand-tuned sharper eta^8 -- is reported, not
+    asserted: it does about as well, since the network mostly learns a
+    sharper preference for near candidates."""
+    import json
+    from vehicleroutingproblem_b200 import prior as PR
+    tr = I.prior_training_instances(256)
+    sols = PR.elite_solutions(tr, ants=64, cand_k=16, epochs=120)
+    with _native.Prior(0, seed=1) as pr:
+        count = pr.set_dataset(tr, [(x[0], x[1]) for x in sols], cand_k=32)
+        losses = pr.train(10, batch=4096, lr=2e-3, seed=11)
+        assert count > 0 and losses[-1] < losses[0]
+        held = I.prior_heldout_instances(4)
+        res = PR.time_to_cost(held, pr, gamma=4.0, epochs=300, ants=256, cand_k=32,
+                              control_beta=8.0)
+    print(json.dumps({"learned_vs_plain_time_ratio": res["time_ratio_of_sums"],
+                      "control_beta8_vs_plain_time_ratio": res["control"]["time_ratio_of_sums"],
+                      "learned_vs_control_final_cost": res["control"][
+                          "learned_vs_control_final_cost_mean"]}))
+    assert res["hit_rate"] == 1.0
+    assert res["time_ratio_of_sums"] < 0.5
 
 
 def test_residual_levels_add_to_plain(dataset, native):

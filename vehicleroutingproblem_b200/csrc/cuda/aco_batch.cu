@@ -54,6 +54,7 @@ struct BatchArgs {
   const float2 *coords;
   const int *demand;
   const uint16_t *cand, *lvl;
+  const uint16_t *tier;      // [rows][kTierLen]: ranks k+1 .. k+64 (fallback)
   const int32_t *A;
   const uint32_t *lut;
   uint8_t *tau;
@@ -182,6 +183,31 @@ __device__ __forceinline__ int seg_nearest(const Seg<LANES> &sg, const SegVisite
   return (mh == 0xffffffffu) ? 0 : (int)mn;
 }
 
+// The fallback of a row none of whose candidates has a weight, exactly as
+// seg_nearest: the first eligible candidate (okm), else the first eligible
+// node of the tier row (the next 64 ranks), else the scan of every node; 0
+// when a complete tier row lists no eligible customer.
+template <int LANES, int V>
+__device__ __forceinline__ int seg_nearest_eligible(const Seg<LANES> &sg,
+                                                    const SegVisited<LANES, V> &vis,
+                                                    const uint16_t *tier_row, unsigned okm, int c,
+                                                    const float2 *coords, const int *dem,
+                                                    bool unit, float2 pc, int room,
+                                                    bool check_dem) {
+  if (okm) return sg.shfl(c, __ffs(okm) - 1);
+  int node = 0;
+#pragma unroll
+  for (int q = 0; q < kTierLen / LANES; ++q) {
+    node = (int)__ldg(tier_row + q * LANES + sg.lane);
+    bool ok = !vis.test(sg, node);  // node 0 (empty slot) reads as visited
+    if (!unit && check_dem && ok) ok = dem[node] <= room;
+    const unsigned m = sg.ballot(ok);
+    if (m) return sg.shfl(node, __ffs(m) - 1);
+  }
+  if (sg.shfl(node, LANES - 1) == 0) return 0;  // every customer was listed
+  return seg_nearest<LANES, V>(sg, vis, coords, dem, unit, pc, room, check_dem);
+}
+
 __device__ __forceinline__ void seg_draw_refill(uint32_t *buf, uint32_t d, uint32_t seed,
                                                 uint32_t epoch, uint32_t ant, int lane,
                                                 int lanes, unsigned mask) {
@@ -253,7 +279,9 @@ __device__ void seg_build_ant(const BatchArgs &a, const BatchInst &I, const Seg<
         if ((d & 127u) == 0u) seg_draw_refill(dbuf, d, seed, epoch, (uint32_t)ant, sg.lane, LANES, sg.mask);
         r_next = dbuf[d & 127u];
       } else {
-        next = seg_nearest<LANES, V>(sg, vis, coords, dem, unit, coords[cur], cap - load, tight);
+        next = seg_nearest_eligible<LANES, V>(
+            sg, vis, a.tier + (size_t)(I.node_off + cur) * kTierLen, sg.ballot(ok), c, coords,
+            dem, unit, coords[cur], cap - load, tight);
         if (next <= 0) break;
       }
       route[pos] = next;
@@ -855,7 +883,7 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
   int *d_order;
   float2 *d_coords;
   int *d_dem;
-  uint16_t *d_cand, *d_lvl;
+  uint16_t *d_cand, *d_lvl, *d_tier;
   int32_t *d_A;
   uint32_t *d_lut;
   float *d_thr;
@@ -871,6 +899,7 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
     // aco_b200_batch_set_cand_k can rebuild them with any length in place.
     b->carve(&d_cand, node * kMaxCand);
     b->carve(&d_lvl, node * kMaxCand);
+    b->carve(&d_tier, node * kTierLen);
     b->carve(&d_A, 256);
     b->carve(&d_lut, 256);
     b->carve(&d_thr, kThresholds);
@@ -914,6 +943,7 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
   BTRY(cudaMemcpyAsync(d_sn, seg_n.data(), sizeof(int) * count, cudaMemcpyHostToDevice, s));
   BTRY(launch_knn_levels_multi(d_coords, d_soff, d_sn, count, node, k, d_thr, kThresholds, d_cand,
                                d_lvl, s));
+  BTRY(launch_knn_tier_multi(d_coords, d_soff, d_sn, count, node, k, d_tier, s));
   b->d_seg_off = d_soff;
   b->d_seg_n = d_sn;
   b->rows = node;
@@ -924,6 +954,7 @@ int aco_b200_batch_setup(aco_b200_batch *b, const aco_b200_batch_problem *p) {
   a.demand = d_dem;
   a.cand = d_cand;
   a.lvl = d_lvl;
+  a.tier = d_tier;
   a.A = d_A;
   a.lut = d_lut;
   BTRY(cudaStreamSynchronize(s));
@@ -1078,6 +1109,8 @@ int aco_b200_batch_set_cand_k(aco_b200_batch *b, int k) {
   BTRY(launch_knn_levels_multi(a.coords, b->d_seg_off, b->d_seg_n, b->count, b->rows, k,
                                b->d_thr, kThresholds, const_cast<uint16_t *>(a.cand),
                                const_cast<uint16_t *>(a.lvl), b->stream));
+  BTRY(launch_knn_tier_multi(a.coords, b->d_seg_off, b->d_seg_n, b->count, b->rows, k,
+                             const_cast<uint16_t *>(a.tier), b->stream));
   b->k = k;
   a.k = k;
   // The launch shape must hold the new list: keep it when it does, else the

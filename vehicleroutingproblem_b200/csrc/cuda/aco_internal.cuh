@@ -166,6 +166,9 @@ cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
                               const float *thr, int J, uint16_t *cand,
                               uint16_t *lvl, cudaStream_t s);
 cudaError_t launch_knn_tier(const float2 *coords, int n, int k, uint16_t *tier, cudaStream_t s);
+cudaError_t launch_knn_tier_multi(const float2 *coords, const long long *seg_off,
+                                  const int *seg_n, int count, long long rows, int k,
+                                  uint16_t *tier, cudaStream_t s);
 // Candidate lists of `count` instances packed one after another: instance s
 // has seg_n[s] customers and starts at row seg_off[s] (device arrays).
 cudaError_t launch_knn_levels_multi(const float2 *coords, const long long *seg_off,

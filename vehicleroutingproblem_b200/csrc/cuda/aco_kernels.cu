@@ -99,6 +99,49 @@ cudaError_t launch_knn_tier(const float2 *coords, int n, int k, uint16_t *tier, 
   return cudaGetLastError();
 }
 
+// Tier lists of many instances in one launch (rows as k_knn_levels_multi):
+// row r of instance s holds what k_knn_tier gives that instance alone.
+__global__ void __launch_bounds__(256) k_knn_tier_multi(
+    const float2 *__restrict__ coords, const long long *__restrict__ seg_off,
+    const int *__restrict__ seg_n, int count, long long rows, int k,
+    uint16_t *__restrict__ tier) {
+  const int lane = threadIdx.x & 31;
+  const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+  const unsigned long long kNone = ~0ull;
+  for (long long r = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows;
+       r += warps) {
+    int lo = 0, hi = count;  // last s with seg_off[s] <= r
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (__ldg(seg_off + mid) <= r) lo = mid; else hi = mid;
+    }
+    const long long off = __ldg(seg_off + lo);
+    const int n = __ldg(seg_n + lo);
+    const int i = (int)(r - off);
+    if (i > n) continue;
+    unsigned long long key = warp_knn(coords + off, n, k, i, lane);
+    int last_lane = k - 1;
+    uint16_t *row = tier + (size_t)r * kTierLen;
+#pragma unroll
+    for (int q = 0; q < kTierLen / 32; ++q) {
+      const unsigned long long last = __shfl_sync(kFull, key, last_lane);
+      key = (last == kNone) ? kNone : warp_knn(coords + off, n, 32, i, lane, last);
+      last_lane = 31;
+      row[32 * q + lane] = (uint16_t)(key == kNone ? 0u : (unsigned)(key & 0xffffffffu));
+    }
+  }
+}
+
+cudaError_t launch_knn_tier_multi(const float2 *coords, const long long *seg_off,
+                                  const int *seg_n, int count, long long rows, int k,
+                                  uint16_t *tier, cudaStream_t s) {
+  if (count < 1 || rows < 1 || k < 1 || k > kMaxCand) return cudaErrorInvalidValue;
+  long long blocks = (rows + 7) / 8;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_knn_tier_multi<<<(int)blocks, 256, 0, s>>>(coords, seg_off, seg_n, count, rows, k, tier);
+  return cudaGetLastError();
+}
+
 // Candidate lists of many instances in one launch.  Instance s owns rows
 // [seg_off[s], seg_off[s] + seg_n[s] + 1) of the concatenated coordinates
 // (seg_off ascending); each warp finds its row's instance by binary search and

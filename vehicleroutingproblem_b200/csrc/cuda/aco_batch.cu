@@ -183,6 +183,10 @@ __device__ __forceinline__ int seg_nearest(const Seg<LANES> &sg, const SegVisite
   return (mh == 0xffffffffu) ? 0 : (int)mn;
 }
 
+// Smallest instance whose fallback uses the tier lists (a lane of a 16-lane
+// segment walks (n+1)/16 bitmap bits in the full scan).
+constexpr int kBatchTierMinCustomers = 256;
+
 // The fallback of a row none of whose candidates has a weight, exactly as
 // seg_nearest: the first eligible candidate (okm), else the first eligible
 // node of the tier row (the next 64 ranks), else the scan of every node; 0
@@ -279,9 +283,12 @@ __device__ void seg_build_ant(const BatchArgs &a, const BatchInst &I, const Seg<
         if ((d & 127u) == 0u) seg_draw_refill(dbuf, d, seed, epoch, (uint32_t)ant, sg.lane, LANES, sg.mask);
         r_next = dbuf[d & 127u];
       } else {
-        next = seg_nearest_eligible<LANES, V>(
-            sg, vis, a.tier + (size_t)(I.node_off + cur) * kTierLen, sg.ballot(ok), c, coords,
-            dem, unit, coords[cur], cap - load, tight);
+        next = (n >= kBatchTierMinCustomers)
+                   ? seg_nearest_eligible<LANES, V>(
+                         sg, vis, a.tier + (size_t)(I.node_off + cur) * kTierLen, sg.ballot(ok),
+                         c, coords, dem, unit, coords[cur], cap - load, tight)
+                   : seg_nearest<LANES, V>(sg, vis, coords, dem, unit, coords[cur], cap - load,
+                                           tight);
         if (next <= 0) break;
       }
       route[pos] = next;

@@ -126,6 +126,8 @@ struct InstanceView {
 };
 
 constexpr int kTierLen = 64;
+// Smallest instance whose construction uses the tier lists.
+constexpr int kTierMinCustomers = 512;
 
 struct AntBuffers {
   int *routes;             // [m][n + 2K] compact routes

@@ -462,7 +462,10 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   iv.demand = ctx->d_demand;
   iv.cand = ctx->d_cand;
   iv.lvl = ctx->d_lvl;
-  iv.tier = ctx->d_tier;
+  // The fallback's tier lists pay for their two L2 round trips only where
+  // the full scan is long (each lane walks (n+1)/32 bitmap bits): at n=1000
+  // the construction takes 279 -> 268 us with them, at n=100 34.2 -> 36.0.
+  iv.tier = (n >= kTierMinCustomers) ? ctx->d_tier : nullptr;
   PheromoneView &pv = ctx->pv;
   pv.tau = ctx->d_tau;
   pv.total = tau_total;

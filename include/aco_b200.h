@@ -409,7 +409,8 @@ ACO_API int aco_b200_evaporate_deposit_noalloc(uint8_t *d_tau, int n, int K,
  * i != j.  iter_deposit and best_deposit are the reference's
  * (weight * Q) / cost values.
  *
- * d_tau: (n+1)^2 doubles, row-major, row stride n+1.  Solutions in compact
+ * d_tau: (n+1)^2 doubles, row-major, row stride n+1, 16-byte aligned (as
+ * cudaMalloc returns it; rejected otherwise).  Solutions in compact
  * form (K segments [0 c.. 0] back to back, K lengths), K <= 8192, device
  * memory.  d_scratch: aco_b200_seq_update_scratch_bytes(n) bytes of device
  * memory, zeroed by the caller before the first call; every call leaves it

@@ -30,7 +30,10 @@ def _many():
     return b.x, b.y, b.demand
 
 
+# (n+1)^2 is odd for even n (the last cell, on the diagonal, is left out of
+# the 16-byte pairs) and even for odd n: both are covered.
 CASES = [("u50", lambda: I.uniform_instance(50, 3, 971), 16),
+         ("u301", lambda: I.uniform_instance(301, 4, 974), 16),
          ("u300_empty_routes", lambda: I.Instance("er", *_many(), 60, 8), 16),
          ("n1000", I.workload_n1000, 32),
          ("u3000", lambda: I.uniform_instance(3000, 12, 973), 32)]
@@ -89,3 +92,6 @@ def test_seq_update_rejects_bad_arguments():
     half = list(args)
     half[6] = ib.data_ptr()  # best nodes without best lengths
     assert L.aco_b200_seq_pheromone_update(*half) == _native.ACO_ERR_INVALID_INPUT
+    odd = list(args)
+    odd[0] = buf.data_ptr() + 8  # not 16-byte aligned
+    assert L.aco_b200_seq_pheromone_update(*odd) == _native.ACO_ERR_INVALID_INPUT

@@ -12,8 +12,9 @@
 // of traffic per cell instead of 32-48), and a small kernel does 2-5 on the
 // touched cells only:
 //   k_seq_mark     sets the bit of every deposit cell (i != j)
-//   k_seq_sweep    rows of the matrix, 4 cells per thread in flight: evaporate;
-//                  unmarked cells also clamp and reset
+//   k_seq_sweep    the matrix two cells (16 bytes) at a time, four pairs per
+//                  thread in flight: evaporate; unmarked cells also clamp
+//                  and reset
 //   k_seq_deposit  one block: the iteration-best adds, then the global-best
 //                  adds (double atomics: the adds to one cell within one
 //                  deposit are of the same amount, so their order does not
@@ -114,37 +115,64 @@ __global__ void __launch_bounds__(1024) k_seq_mark(SeqArgs a) {
   }
 }
 
+// The matrix as a flat array of (n+1)^2 cells taken two at a time (16-byte
+// loads and stores; the matrix starts 16-byte aligned): cell e is on the
+// diagonal exactly when e mod (n+2) == 0, and its mark is bit e mod 32 of
+// word e / 32 (both cells of a pair share the word).
+__device__ __forceinline__ bool on_diagonal(unsigned long long e, unsigned long long n2,
+                                            double inv_n2) {
+  // e / n2 from the FP64 reciprocal, corrected to the exact quotient
+  long long q = (long long)((double)e * inv_n2);
+  long long r = (long long)e - q * (long long)n2;
+  if (r < 0) r += (long long)n2;
+  if (r >= (long long)n2) r -= (long long)n2;
+  return r == 0;
+}
+
+__device__ __forceinline__ double sweep_cell(double x, unsigned long long e, unsigned int word,
+                                             unsigned long long n2, double inv_n2,
+                                             const SeqArgs &a) {
+  if (on_diagonal(e, n2, inv_n2)) return x;
+  double y = __dmul_rn(x, a.keep);
+  if (!((word >> (e & 31)) & 1u)) y = clamp_reset(y, a);
+  return y;
+}
+
 __global__ void __launch_bounds__(kSweepThreads) k_seq_sweep(SeqArgs a) {
-  const int rows = a.n + 1;
-  const int span = kSweepUnroll * blockDim.x;
-  for (int i = blockIdx.x; i < rows; i += gridDim.x) {
-    double *row = a.tau + (size_t)i * rows;
-    const unsigned long long row0 = (unsigned long long)i * rows;
-    for (int j0 = threadIdx.x; j0 < rows; j0 += span) {
-      double x[kSweepUnroll];
-      unsigned int m[kSweepUnroll];
+  const unsigned long long cells = (unsigned long long)(a.n + 1) * (unsigned long long)(a.n + 1);
+  const unsigned long long n2 = (unsigned long long)a.n + 2;
+  const double inv_n2 = 1.0 / (double)n2;
+  const unsigned long long nvec = cells / 2;
+  double2 *t2 = reinterpret_cast<double2 *>(a.tau);
+  const unsigned long long tile = (unsigned long long)kSweepUnroll * blockDim.x;
+  const unsigned long long step = tile * gridDim.x;
+  for (unsigned long long base = blockIdx.x * tile + threadIdx.x; base < nvec; base += step) {
+    double2 v[kSweepUnroll];
+    unsigned int m[kSweepUnroll];
 #pragma unroll
-      for (int q = 0; q < kSweepUnroll; ++q) {
-        const int j = j0 + q * blockDim.x;
-        x[q] = 0.0;
-        m[q] = 0u;
-        if (j < rows) {
-          x[q] = __ldcs(row + j);
-          const unsigned long long c = row0 + j;
-          m[q] = (__ldg(a.marks + (c >> 5)) >> (c & 31)) & 1u;
-        }
+    for (int q = 0; q < kSweepUnroll; ++q) {
+      const unsigned long long i = base + (unsigned long long)q * blockDim.x;
+      v[q] = make_double2(0.0, 0.0);
+      m[q] = 0u;
+      if (i < nvec) {
+        v[q] = __ldcs(t2 + i);
+        m[q] = __ldg(a.marks + ((2 * i) >> 5));
       }
+    }
 #pragma unroll
-      for (int q = 0; q < kSweepUnroll; ++q) {
-        const int j = j0 + q * blockDim.x;
-        if (j < rows && j != i) {
-          double y = __dmul_rn(x[q], a.keep);
-          if (!m[q]) y = clamp_reset(y, a);
-          __stcs(row + j, y);
-        }
+    for (int q = 0; q < kSweepUnroll; ++q) {
+      const unsigned long long i = base + (unsigned long long)q * blockDim.x;
+      if (i < nvec) {
+        const unsigned long long e = 2 * i;
+        double2 r;
+        r.x = sweep_cell(v[q].x, e, m[q], n2, inv_n2, a);
+        r.y = sweep_cell(v[q].y, e + 1, m[q], n2, inv_n2, a);
+        __stcs(t2 + i, r);
       }
     }
   }
+  // An odd cell count leaves the last cell, (n, n), out of the pairs: it is
+  // on the diagonal, which the update never changes.
 }
 
 __global__ void __launch_bounds__(1024) k_seq_deposit(SeqArgs a) {
@@ -208,6 +236,10 @@ extern "C" ACO_API int aco_b200_seq_pheromone_update(
     fprintf(stderr, "aco_b200_seq_pheromone_update: invalid arguments\n");
     return ACO_ERR_INVALID_INPUT;
   }
+  if (((uintptr_t)d_tau & 15u) != 0u) {
+    fprintf(stderr, "aco_b200_seq_pheromone_update: d_tau must be 16-byte aligned\n");
+    return ACO_ERR_INVALID_INPUT;
+  }
   SeqArgs a;
   a.tau = d_tau;
   a.n = n;
@@ -229,8 +261,12 @@ extern "C" ACO_API int aco_b200_seq_pheromone_update(
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  int grid = sms * 8;
-  if (grid > n + 1) grid = n + 1;
+  const unsigned long long pairs = (unsigned long long)(n + 1) * (unsigned long long)(n + 1) / 2;
+  const unsigned long long per_block = (unsigned long long)kSweepUnroll * kSweepThreads;
+  unsigned long long g = (pairs + per_block - 1) / per_block;
+  if (g > (unsigned long long)sms * 8) g = (unsigned long long)sms * 8;
+  if (g < 1) g = 1;
+  const int grid = (int)g;
   k_seq_mark<<<1, 1024, smem, s>>>(a);
   k_seq_sweep<<<grid, kSweepThreads, 0, s>>>(a);
   k_seq_deposit<<<1, 1024, smem, s>>>(a);

@@ -622,10 +622,9 @@ __device__ void build_ant(const ConstructArgs &a, const Tables<L, UNIT> &tb,
       tight = !UNIT && load > tight_load;
       cur = nx;
     };
-    // Two steps per loop trip give the scheduler one step's bookkeeping to
-    // interleave with the next step's chain (measured: 304 -> 302 us at
-    // n=1000, 883 -> 868 us at n=2000; four steps were slower).
-#pragma unroll 2
+    // One step per loop trip (unrolling by two was 0.9 % slower at n=1000
+    // once the prefix came from independent shuffles).
+#pragma unroll 1
     while (rem_dem > limit && load < cap) {
       const bool may_close = CREF && rem_dem <= future;
       if (CREF && may_close && cur == 0) break;

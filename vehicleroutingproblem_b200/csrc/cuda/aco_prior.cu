@@ -66,8 +66,11 @@ constexpr uint32_t kSBar = kSRed + 4 * 65 * 4 + 48;    // mbarrier, TMEM base
 constexpr uint32_t kSmemTrain = kSBar + 64;
 constexpr uint32_t kSmemForward = kSmemTrain;         // same layout, training parts unused
 
-// Tensor-memory columns: Z1 0-63, Z2 64-127, dH1 128-191, dW 192-271.
-constexpr uint32_t kColZ1 = 0, kColZ2 = 64, kColDH1 = 128, kColDW = 192;
+// Tensor-memory columns: Z1 0-63, Z2 64-127, dW 128-207.  dH1 goes into
+// Z2's columns: Z2 is read for the last time (the dZ2 epilogue) before the
+// dH1 MMA is issued.  Training thus fits 256 columns, half of an SM's
+// tensor memory, and two training blocks share an SM.
+constexpr uint32_t kColZ1 = 0, kColZ2 = 64, kColDH1 = 64, kColDW = 128;
 
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
@@ -220,7 +223,7 @@ struct MlpArgs {
 };
 
 template <bool TRAIN>
-__global__ void __launch_bounds__(128, 1) k_prior_mlp(MlpArgs a) {
+__global__ void __launch_bounds__(128, 2) k_prior_mlp(MlpArgs a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char *sB1 = smem + kSB1, *sB2 = smem + kSB2, *sB2T = smem + kSB2T;
   unsigned char *sA1 = smem + kSA1, *sA2 = smem + kSA2, *sAdw = smem + kSAdw, *sBdw = smem + kSBdw;
@@ -229,7 +232,7 @@ __global__ void __launch_bounds__(128, 1) k_prior_mlp(MlpArgs a) {
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem + kSBar);
   uint32_t *s_tmem = reinterpret_cast<uint32_t *>(smem + kSBar + 8);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  constexpr uint32_t kCols = TRAIN ? 512u : 128u;
+  constexpr uint32_t kCols = TRAIN ? 256u : 128u;
 
   if (warp == 0) {
     umma::tmem_alloc(s_tmem, kCols);
@@ -592,7 +595,7 @@ struct aco_b200_prior {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   float *d_params = nullptr, *d_m = nullptr, *d_v = nullptr, *d_grad = nullptr, *d_loss = nullptr;
-  float *d_gpart = nullptr;  // [num_sms][kGradStride] partial gradients
+  float *d_gpart = nullptr;  // [2 num_sms][kGradStride] partial gradients
   int *d_error = nullptr;
   int adam_step = 0;
   // training set
@@ -740,7 +743,8 @@ int aco_b200_prior_create(aco_b200_prior **out, int device) {
       cudaMalloc(&p->d_v, pb) != cudaSuccess || cudaMalloc(&p->d_grad, pb) != cudaSuccess ||
       cudaMalloc(&p->d_loss, 16) != cudaSuccess || cudaMalloc(&p->d_error, 16) != cudaSuccess ||
       cudaMalloc(&p->d_radius, 16) != cudaSuccess ||
-      cudaMalloc(&p->d_gpart, (size_t)p->num_sms * kGradStride * sizeof(float)) != cudaSuccess) {
+      cudaMalloc(&p->d_gpart, (size_t)2 * p->num_sms * kGradStride * sizeof(float)) !=
+          cudaSuccess) {
     delete p;
     return ACO_ERR_ALLOCATION;
   }
@@ -980,7 +984,9 @@ static int run_gradient(aco_b200_prior *p, const int *order, int count, cudaStre
   a.gpart = p->d_gpart;
   a.error = p->d_error;
   a.tiles = (count + 3) / 4;
-  const int grid = std::max(1, std::min(a.tiles, p->num_sms));
+  // Two training blocks per SM (256 tensor-memory columns and 94 KB of shared
+  // memory each): one block's MMA runs while the other's epilogue does.
+  const int grid = std::max(1, std::min(a.tiles, p->num_sms * 2));
   k_prior_mlp<true><<<grid, 128, kSmemTrain, s>>>(a);
   PTRY(cudaGetLastError());
   k_prior_reduce<<<(kParams + 1 + 255) / 256, 256, 0, s>>>(p->d_gpart, grid, p->d_grad, p->d_loss);

@@ -43,7 +43,8 @@ solver, same CLI contract, same GPU, unit-demand twin of n1000.
   batched form on the full 512-instance batch beside the single-instance
   solver looped over a sample, and the learned prior's time-to-cost against
   plain eta (and a tuned-beta control) with 512 training and 8 held-out
-  instances.
+  instances; other_configs: the small and clustered2000 workloads over 50
+  epochs each beside the reference's OpenMP solver.
 * cli_same_contract / reference_cuda_same_gpu (reference arm): this
   library's aco_vrp_cuda.out and the reference's own CUDA solver (built from
   its sources for sm_100a) run through the same CLI on the same GPU and the
@@ -690,6 +691,7 @@ def run_single(args, rank, world, local, torch, dist, _native):
             line["roofline_seq_update_hbm"] = roof_seq_hbm
         if world == 1 and args.workload == "n1000" and not args.no_extras:
             line.update(default_extras(local, torch, _native))
+            line["other_configs"] = other_configs(local, torch, _native, args.no_cpu_baseline)
         if world == 1 and not args.no_cpu_baseline:
             try:
                 line["cpu_baseline"] = cpu_baseline(inst, m, cand_k=k)
@@ -1063,6 +1065,40 @@ def run_learned(args, rank, world, local, torch, dist, _native):
         "per_instance_sample": rows[:4],
     }
     return line
+
+
+def other_configs(local, torch, _native, no_cpu):
+    """The two other single-instance configurations the CPU comparison is
+    quoted on, on bounded samples: the small n=100 and the clustered n=2000
+    workloads, device ant-steps/s over 50 epochs (CUDA events, L2 flushed
+    between epochs) beside the reference's OpenMP solver on the host cores."""
+    out = {}
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    for name in ("small", "clustered2000"):
+        wl = WORKLOADS[name]
+        inst = wl["factory"]()
+        try:
+            with _native.Context(local) as ctx:
+                ctx.set_stream(stream.cuda_stream)
+                ctx.setup_instance(inst, ants=wl["ants"], cand_k=wl["cand_k"], seed=1234)
+                ctx.enqueue_epochs(5)
+                torch.cuda.synchronize()
+                s0 = ctx.state().total_steps
+                steps = 50
+                ms = timed_steps(torch, stream, steps, lambda: ctx.enqueue_epochs(1), flush)
+                done = ctx.state().total_steps - s0
+            r = {"workload": wl["name"], "value": done / (ms / 1e3), "unit": "ant-steps/s",
+                 "ms_per_step": ms / steps, "steps": steps, "warmup": 5}
+            if not no_cpu:
+                r["cpu_baseline"] = cpu_baseline(inst, wl["ants"], target_s=6.0,
+                                                 cand_k=wl["cand_k"])
+                r["vs_cpu_baseline"] = r["value"] / r["cpu_baseline"]["value"]
+            out[name] = r
+        except Exception as exc:  # reported, not fatal
+            out[name] = {"error": str(exc)[:300]}
+    return out
 
 
 def default_extras(local, torch, _native):

@@ -381,12 +381,13 @@ struct Visited {
     }
     // Lane c mod 32 holds node c (the shuffle takes the source modulo 32),
     // at bit (c / 32) mod 32.
+    const uint32_t bit = __funnelshift_l(0u, 1u, c >> 5);  // formed while the shuffle flies
     uint32_t word = __shfl_sync(kFull, w0, c);
     if (V == 2) {
       const uint32_t hi = __shfl_sync(kFull, w1, c);
       word = (c >> 10) ? hi : word;
     }
-    return (__funnelshift_r(word, word, c >> 5) & 1u) != 0u;
+    return (word & bit) != 0u;
   }
   __device__ __forceinline__ void set(int node, int lane) {
     if (V == 0) {

@@ -163,8 +163,9 @@ def ablation(train: int = 2048, val: int = 12, epochs: int = 300, device: int = 
     """Final cost relative to the plain solver (beta = 2) on validation
     instances (n=1000, K=8, seeds 60000..): the plain solver with sharper
     hand-set eta^beta, and priors trained on elite routes of the plain solver
-    at beta 2 and 8, their levels replacing (pure) or added to (residual) the
-    plain levels.  Yields one dict per configuration."""
+    at beta 2 and 8, their levels replacing (pure) or added to (residual,
+    on plain levels of beta 2, 5 or 8) the plain levels.  Yields one dict
+    per configuration."""
     tr = I.prior_training_instances(train)
     vs = [I.uniform_instance(1000, 8, 60000 + i) for i in range(val)]
     base = final_costs(vs, epochs, device=device)
@@ -184,8 +185,8 @@ def ablation(train: int = 2048, val: int = 12, epochs: int = 300, device: int = 
             for g in (1.0, 2.0, 4.0):
                 yield row(f"learned (elites beta={eb:g}) pure gamma={g:g}",
                           final_costs(vs, epochs, pr, g, device=device), **info)
-            for g in (1.0, 2.0):
-                for pb in (2.0, 5.0):
+            for g in (0.5, 1.0, 2.0):
+                for pb in (2.0, 5.0, 8.0):
                     yield row(f"learned (elites beta={eb:g}) residual gamma={g:g} beta={pb:g}",
                               final_costs(vs, epochs, pr, g, True, pb, device=device), **info)
 

@@ -976,19 +976,24 @@ LEARNED = dict(train=4096, heldout=256, elite_ants=64, elite_k=16, elite_epochs=
 TRAIN_FLOPS_PER_EDGE = 2 * (8 * 64 + 64 * 64 + 64) + 2 * (64 * 64 + 64 * 64 + 8 * 64 + 64)
 
 
-def learned_measure(local, torch, _native, ntrain, nheld, nval):
+def learned_measure(local, torch, _native, ntrain, nheld, nval, elite_beta=2.0,
+                    residual_beta=None, gammas=None):
     """The learned prior's whole pipeline on one GPU: elite routes of the
     plain batched solver on `ntrain` training instances, the training set,
     tensor-core training, gamma for the learned levels and the beta of a
     control (the plain solver with a sharper hand-set eta^beta) each chosen
     on `nval` validation instances by mean final cost relative to the plain
-    solver, then time-to-cost on `nheld` held-out n=1000 instances."""
+    solver, then time-to-cost on `nheld` held-out n=1000 instances.
+    elite_beta: eta^beta of the plain solver that makes the elite routes;
+    residual_beta: the learned levels are added to plain eta^residual_beta
+    levels (None: they replace the plain levels)."""
     from vehicleroutingproblem_b200 import prior as PR
     L = LEARNED
+    gammas = gammas or L["gammas"]
     tr = I.prior_training_instances(ntrain)
     t0 = time.perf_counter()
     sols = PR.elite_solutions(tr, ants=L["elite_ants"], cand_k=L["elite_k"],
-                              epochs=L["elite_epochs"])
+                              epochs=L["elite_epochs"], beta=elite_beta)
     elite_s = time.perf_counter() - t0
     pr = _native.Prior(local, seed=1)
     try:
@@ -1001,9 +1006,11 @@ def learned_measure(local, torch, _native, ntrain, nheld, nval):
         train_s = time.perf_counter() - t0
         val = [I.uniform_instance(1000, 8, 60000 + i) for i in range(nval)]
         base = PR.final_costs(val, L["epochs"], ants=L["ants"], cand_k=L["cand_k"])
+        res_kw = ({} if residual_beta is None else
+                  {"residual": True, "beta": residual_beta})
         scores = {g: float(np.mean(PR.final_costs(val, L["epochs"], pr, g, ants=L["ants"],
-                                                  cand_k=L["cand_k"]) / base))
-                  for g in L["gammas"]}
+                                                  cand_k=L["cand_k"], **res_kw) / base))
+                  for g in gammas}
         gamma = min(scores, key=lambda g: scores[g])
         ctrl = {b: float(np.mean(PR.final_costs(val, L["epochs"], beta=b, ants=L["ants"],
                                                 cand_k=L["cand_k"]) / base))
@@ -1012,7 +1019,8 @@ def learned_measure(local, torch, _native, ntrain, nheld, nval):
         held = I.prior_heldout_instances(nheld)
         t0 = time.perf_counter()
         res = PR.time_to_cost(held, pr, gamma=gamma, epochs=L["epochs"], ants=L["ants"],
-                              cand_k=L["cand_k"], control_beta=beta_c)
+                              cand_k=L["cand_k"], control_beta=beta_c,
+                              residual_beta=residual_beta)
         eval_s = time.perf_counter() - t0
     finally:
         pr.close()
@@ -1030,7 +1038,10 @@ def run_learned(args, rank, world, local, torch, dist, _native):
     L = LEARNED
     ntrain = args.prior_train or L["train"]
     nheld = args.prior_heldout or L["heldout"]
-    r = learned_measure(local, torch, _native, ntrain, nheld, L["validation"])
+    gammas = tuple(float(x) for x in args.prior_gammas.split(",")) if args.prior_gammas else None
+    r = learned_measure(local, torch, _native, ntrain, nheld, L["validation"],
+                        elite_beta=args.prior_elite_beta, residual_beta=args.prior_residual_beta,
+                        gammas=gammas)
     res = r["res"]
     rows = res.pop("rows")
     peak, peak_kind = None, "fallback"
@@ -1048,6 +1059,9 @@ def run_learned(args, rank, world, local, torch, dist, _native):
         "dtype": "bf16 MLP (fp32 accumulate) + int32 weights + u8 pheromone",
         "data": "synthetic",
         "config": {"workload": L["name"], "train_instances": ntrain, "heldout": nheld,
+                   "elite_beta": args.prior_elite_beta,
+                   "levels": ("learned, replacing plain eta" if args.prior_residual_beta is None
+                              else f"learned, added to plain eta^{args.prior_residual_beta:g}"),
                    "gamma": r["gamma"], "gamma_validation_final_cost": r["scores"],
                    "control_beta": r["beta_c"], "control_validation_final_cost": r["ctrl"]},
         "time_to_cost": res,
@@ -1164,6 +1178,12 @@ def main():
                     help="learned: training instances (default 4096)")
     ap.add_argument("--prior-heldout", type=int, default=None,
                     help="learned: held-out instances (default 256)")
+    ap.add_argument("--prior-elite-beta", type=float, default=2.0,
+                    help="learned: eta^beta of the plain solver making the elite routes")
+    ap.add_argument("--prior-residual-beta", type=float, default=None,
+                    help="learned: add the learned levels to plain eta^beta levels")
+    ap.add_argument("--prior-gammas", default=None,
+                    help="learned: comma-separated gammas to choose from on validation")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--looped-sample", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")

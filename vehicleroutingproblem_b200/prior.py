@@ -55,9 +55,10 @@ def train_prior(prior: "N.Prior", instances, solutions, epochs: int = 8, batch: 
 
 def convergence(inst: I.Instance, epochs: int, prior: Optional["N.Prior"] = None,
                 gamma: float = 1.0, ants: int = 256, cand_k: int = 32, seed: int = 1234,
-                device: int = 0, beta: float = 2.0):
+                device: int = 0, beta: float = 2.0, residual: bool = False):
     """Best cost after every epoch, the device time (s) at every epoch (from
-    the first epoch's start) and the seconds spent applying the prior."""
+    the first epoch's start) and the seconds spent applying the prior
+    (residual: its levels added to the plain eta^beta levels)."""
     import torch
     s = torch.cuda.Stream(device)
     with N.Context(device) as c:
@@ -68,7 +69,7 @@ def convergence(inst: I.Instance, epochs: int, prior: Optional["N.Prior"] = None
         if prior is not None:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(s)
-            c.apply_prior(prior, gamma)
+            c.apply_prior(prior, gamma, residual=residual)
             e1.record(s)
             e1.synchronize()
             t_prior = e0.elapsed_time(e1) / 1e3
@@ -89,16 +90,22 @@ def _time_to(best, t, target, extra=0.0):
 
 def time_to_cost(heldout: Sequence[I.Instance], prior: "N.Prior", gamma: float = 1.0,
                  epochs: int = 300, ants: int = 256, cand_k: int = 32, tol: float = 0.005,
-                 seed: int = 1234, device: int = 0, control_beta: Optional[float] = None) -> Dict:
+                 seed: int = 1234, device: int = 0, control_beta: Optional[float] = None,
+                 residual_beta: Optional[float] = None) -> Dict:
     """Per held-out instance: the plain solver's final cost C after `epochs`
     epochs, the target (1 + tol) C, and the time each solver first reaches
     it (the learned one pays its inference time too).  control_beta: also
     the plain solver with eta^control_beta (a sharper hand-set heuristic)
-    against the same target."""
+    against the same target.  residual_beta: the learned levels are added to
+    the plain eta^residual_beta levels instead of replacing the plain ones."""
     rows = []
     for j, inst in enumerate(heldout):
         bp, tp, _ = convergence(inst, epochs, None, gamma, ants, cand_k, seed + j, device)
-        bl, tl, t_inf = convergence(inst, epochs, prior, gamma, ants, cand_k, seed + j, device)
+        if residual_beta is None:
+            bl, tl, t_inf = convergence(inst, epochs, prior, gamma, ants, cand_k, seed + j, device)
+        else:
+            bl, tl, t_inf = convergence(inst, epochs, prior, gamma, ants, cand_k, seed + j, device,
+                                        beta=residual_beta, residual=True)
         target = bp[-1] * (1.0 + tol)
         ep, sp, _ = _time_to(bp, tp, target)
         el, sl, hit = _time_to(bl, tl, target, t_inf)

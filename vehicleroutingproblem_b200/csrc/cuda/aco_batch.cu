@@ -199,16 +199,20 @@ __device__ __forceinline__ int seg_nearest_eligible(const Seg<LANES> &sg,
                                                     bool unit, float2 pc, int room,
                                                     bool check_dem) {
   if (okm) return sg.shfl(c, __ffs(okm) - 1);
-  int node = 0;
+  int nodes[kTierLen / LANES];
+#pragma unroll
+  for (int q = 0; q < kTierLen / LANES; ++q)  // every part of the row in flight at once
+    nodes[q] = (int)__ldg(tier_row + q * LANES + sg.lane);
 #pragma unroll
   for (int q = 0; q < kTierLen / LANES; ++q) {
-    node = (int)__ldg(tier_row + q * LANES + sg.lane);
+    const int node = nodes[q];
     bool ok = !vis.test(sg, node);  // node 0 (empty slot) reads as visited
     if (!unit && check_dem && ok) ok = dem[node] <= room;
     const unsigned m = sg.ballot(ok);
     if (m) return sg.shfl(node, __ffs(m) - 1);
   }
-  if (sg.shfl(node, LANES - 1) == 0) return 0;  // every customer was listed
+  // every customer was listed
+  if (sg.shfl(nodes[kTierLen / LANES - 1], LANES - 1) == 0) return 0;
   return seg_nearest<LANES, V>(sg, vis, coords, dem, unit, pc, room, check_dem);
 }
 

@@ -449,16 +449,20 @@ __device__ __forceinline__ int nearest_eligible(const Tables<L, UNIT> &tb, const
   if (okm) return __shfl_sync(kFull, c, __ffs(okm) - 1);
   if (tb.tier) {
     const uint16_t *row = tb.tier + (size_t)cur * kTierLen;
-    int node = 0;
+    int nodes[kTierLen / 32];
+#pragma unroll
+    for (int r = 0; r < kTierLen / 32; ++r)  // both halves in flight at once
+      nodes[r] = (int)__ldg(row + 32 * r + lane);
 #pragma unroll
     for (int r = 0; r < kTierLen / 32; ++r) {
-      node = (int)__ldg(row + 32 * r + lane);
+      const int node = nodes[r];
       bool ok = !vis.test(node);  // node 0 (empty slot) reads as visited
       if (!UNIT && check_dem && ok) ok = tb.demand(node) <= room;
       const unsigned m = __ballot_sync(kFull, ok);
       if (m) return __shfl_sync(kFull, node, __ffs(m) - 1);
     }
-    if (__shfl_sync(kFull, node, 31) == 0) return 0;  // every customer was listed
+    // every customer was listed
+    if (__shfl_sync(kFull, nodes[kTierLen / 32 - 1], 31) == 0) return 0;
   }
   return nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), room, check_dem, lane);
 }

@@ -412,25 +412,65 @@ __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
                                                  float2 pc, int room,
                                                  bool check_dem, int lane) {
   uint32_t best_h = 0xffffffffu, best_n = 0xffffffffu;
-  // V = 1, 2: bit b of a register word is node first + 32 b (ascending);
-  // V = 0: bit b of word wi is node 32 wi + b.
-  auto scan = [&](uint32_t fr, int first, int step) {
-    while (fr) {
-      const int b = __ffs(fr) - 1;
-      fr &= fr - 1;
-      const int node = first + b * step;
-      if (!UNIT && check_dem && tb.demand(node) > room) continue;
-      const uint32_t h = __float_as_uint(dist2f(pc, tb.coord(node)));
-      if (h < best_h) {
-        best_h = h;
-        best_n = (uint32_t)node;
-      }
+  auto visit = [&](int node, float2 p, int dem) {
+    if (!UNIT && check_dem && dem > room) return;
+    const uint32_t h = __float_as_uint(dist2f(pc, p));
+    if (h < best_h) {
+      best_h = h;
+      best_n = (uint32_t)node;
     }
   };
-  if (V >= 1) scan(~vis.w0, lane, 32);
-  if (V == 2) scan(~vis.w1, 1024 + lane, 32);
-  if (V == 0)
-    for (int wi = lane; wi < vis.vw; wi += 32) scan(~vis.s[wi], wi << 5, 1);
+  if (V >= 1) {
+    // Bit b of register word j is node 1024 j + lane + 32 b (ascending);
+    // the tables are in shared memory, so one node at a time.
+    auto scan = [&](uint32_t fr, int first) {
+      while (fr) {
+        const int b = __ffs(fr) - 1;
+        fr &= fr - 1;
+        const int node = first + b * 32;
+        if (!UNIT && check_dem && tb.demand(node) > room) continue;
+        visit(node, tb.coord(node), 0);
+      }
+    };
+    scan(~vis.w0, lane);
+    if (V == 2) scan(~vis.w1, 1024 + lane);
+  } else {
+    // Words wi = lane + 32 j of the bitmap, bit b node 32 wi + b.  The
+    // unvisited nodes are taken kScanBatch at a time and their coordinate
+    // (and demand) loads issued together, so a lane waits once per batch
+    // rather than once per node; they are still compared in ascending order.
+    constexpr int kScanBatch = 16;
+    const int nwords = lane < vis.vw ? (vis.vw - 1 - lane) / 32 + 1 : 0;
+    int j = 0;
+    uint32_t fr = nwords > 0 ? ~vis.s[lane] : 0u;
+    while (true) {
+      int nd[kScanBatch];
+#pragma unroll
+      for (int q = 0; q < kScanBatch; ++q) {
+        while (fr == 0u && ++j < nwords) fr = ~vis.s[lane + 32 * j];
+        nd[q] = -1;
+        if (fr) {
+          nd[q] = ((lane + 32 * j) << 5) + __ffs(fr) - 1;
+          fr &= fr - 1;
+        }
+      }
+      float2 pq[kScanBatch];
+      int dq[kScanBatch];
+#pragma unroll
+      for (int q = 0; q < kScanBatch; ++q) {
+        pq[q] = make_float2(0.f, 0.f);
+        dq[q] = 0;
+        if (nd[q] >= 0) {
+          pq[q] = tb.coord(nd[q]);
+          if (!UNIT && check_dem) dq[q] = tb.demand(nd[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kScanBatch; ++q)
+        if (nd[q] >= 0) visit(nd[q], pq[q], dq[q]);
+      if (nd[kScanBatch - 1] < 0) break;
+    }
+  }
   const uint32_t mh = __reduce_min_sync(kFull, best_h);
   const uint32_t mn = __reduce_min_sync(kFull, best_h == mh ? best_n : 0xffffffffu);
   return (mh == 0xffffffffu) ? 0 : (int)mn;

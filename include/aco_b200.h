@@ -206,6 +206,14 @@ ACO_API int aco_b200_evaporate_deposit(aco_b200_ctx *ctx, int best_ant,
 ACO_API int aco_b200_shard_packet_ints(aco_b200_ctx *ctx);
 ACO_API int aco_b200_shard_construct(aco_b200_ctx *ctx, int32_t *d_send);
 ACO_API int aco_b200_shard_update(aco_b200_ctx *ctx, const int32_t *d_recv, int world);
+/* A number that changes whenever a set-up changes the arguments the
+ * context's launches are recorded with (sizes, parameters, buffers; -1 if
+ * not set up).  The shard calls above only enqueue launches, so a caller may
+ * record steps 1-3 of whole epochs in a CUDA graph of its own (stream
+ * capture on the context stream, its all-gather included); it re-records
+ * when this number changes.  Graph replays read the epoch number from the
+ * device state. */
+ACO_API int aco_b200_graph_generation(aco_b200_ctx *ctx);
 
 /*
  * Learned heuristic prior.  A small MLP (8 candidate-edge features -> 64 ->

@@ -2,6 +2,9 @@
 the ants.  One GPU stands in for the devices: two contexts with ant_base 0
 and m exchange their packets through a device buffer, epoch by epoch, and
 must follow one context with 2m ants exactly (pheromone, state, best)."""
+import contextlib
+import datetime
+
 import numpy as np
 import pytest
 
@@ -158,21 +161,75 @@ def test_shards_without_a_feasible_ant(native):
         c.close()
 
 
-def test_sharded_colony_over_nccl_world_one(native):
-    """ShardedColony through a real NCCL process group (one rank) follows the
-    plain context epoch for epoch."""
+@contextlib.contextmanager
+def _nccl_world_one():
     import os
     import socket
     import torch
     import torch.distributed as dist
-    inst = I.uniform_instance(200, 5, 775)
     with socket.socket() as sk:
         sk.bind(("127.0.0.1", 0))
         port = sk.getsockname()[1]
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0))
+    dist.init_process_group("nccl", rank=0, world_size=1, device_id=torch.device("cuda", 0),
+                            timeout=datetime.timedelta(seconds=60))
     try:
+        yield
+    finally:
+        dist.destroy_process_group()
+
+
+def _same_colony(a, b):
+    sa, sb = a.state(), b.state()
+    assert (sa.epochs, sa.found, sa.best_ant, sa.iter_since_best, sa.total_steps, sa.error) == \
+        (sb.epochs, sb.found, sb.best_ant, sb.iter_since_best, sb.total_steps, 0)
+    assert sa.global_best == sb.global_best and sa.iter_best == sb.iter_best
+    assert np.array_equal(a.tau(), b.tau())
+    (an, al, ac), (bn, bl, bc) = a.best(), b.best()
+    assert ac == bc and np.array_equal(al, bl) and np.array_equal(an, bn)
+
+
+def test_sharded_colony_graphs_follow_eager_epochs(native):
+    """Epochs replayed from the recorded graphs (1 and 16 epochs, the NCCL
+    all-gather inside) equal epochs launched one call at a time, and a set-up
+    with other sizes re-records them."""
+    import torch
+    with _nccl_world_one():
+        inst = I.uniform_instance(200, 5, 776)
+        a = S.ShardedColony(inst, 48, 0, cand_k=16, seed=7, graphs=True)
+        b = S.ShardedColony(inst, 48, 0, cand_k=16, seed=7, graphs=False)
+        try:
+            for e in (1, 16, 3, 17):
+                a.enqueue_epochs(e)
+                a.stream.synchronize()
+                b.enqueue_epochs(e)
+                b.stream.synchronize()
+                _same_colony(a, b)
+            assert len(a._graphs) == 2 and not b._graphs
+            g0 = a.ctx.graph_generation()
+            inst2 = I.uniform_instance(260, 6, 777)
+            for c in (a, b):
+                c.setup(inst2, cand_k=16, seed=8)
+            assert a.ctx.graph_generation() != g0
+            a.enqueue_epochs(18)
+            a.stream.synchronize()
+            b.enqueue_epochs(18)
+            b.stream.synchronize()
+            _same_colony(a, b)
+            assert a.state().epochs == 18 and len(a._graphs) == 2
+        finally:
+            a.close()
+            b.close()
+        torch.cuda.synchronize()
+
+
+def test_sharded_colony_over_nccl_world_one(native):
+    """ShardedColony through a real NCCL process group (one rank) follows the
+    plain context epoch for epoch."""
+    import torch
+    inst = I.uniform_instance(200, 5, 775)
+    with _nccl_world_one():
         col = S.ShardedColony(inst, 48, 0, cand_k=16, seed=5)
         st = col.run(37, chunk=16)
         ref = _setup(native, inst, 16, 48, 0, torch.cuda.Stream(), seed=5)
@@ -184,5 +241,3 @@ def test_sharded_colony_over_nccl_world_one(native):
         assert len(pk) == 1 and pk[0].found and pk[0].global_ant == st_r.best_ant
         col.close()
         ref.close()
-    finally:
-        dist.destroy_process_group()

@@ -41,6 +41,7 @@ EXPORTED = [
     "aco_b200_batch_solve", "aco_b200_batch_enqueue", "aco_b200_batch_synchronize",
     "aco_b200_batch_get", "aco_b200_batch_get_costs", "aco_b200_batch_get_all",
     "aco_b200_shard_packet_ints", "aco_b200_shard_construct", "aco_b200_shard_update",
+    "aco_b200_graph_generation",
     "aco_b200_get_depot_tables", "aco_b200_debug_inject", "aco_b200_construct_with_draws",
     "aco_b200_prior_create", "aco_b200_prior_destroy", "aco_b200_prior_set_stream",
     "aco_b200_prior_init", "aco_b200_prior_set_params", "aco_b200_prior_get_params",
@@ -143,7 +144,7 @@ def load():
         "aco_b200_batch_get_all": [vp, vp, vp, vp],
         "aco_b200_batch_get_costs": [vp, vp, vp, vp],
         "aco_b200_shard_packet_ints": [vp], "aco_b200_shard_construct": [vp, vp],
-        "aco_b200_shard_update": [vp, vp, i32],
+        "aco_b200_shard_update": [vp, vp, i32], "aco_b200_graph_generation": [vp],
         "aco_b200_get_depot_tables": [vp, vp, vp, vp],
         "aco_b200_debug_inject": [vp, i32, i32],
         "aco_b200_construct_with_draws": [vp, vp, i32],
@@ -392,6 +393,12 @@ class Context:
         if P < 0:
             raise AcoError(ACO_ERR_INVALID_INPUT, "aco_b200_shard_packet_ints")
         return P
+
+    def graph_generation(self) -> int:
+        """Changes whenever a set-up changes the arguments the context's
+        launches are recorded with; graphs recorded around its launches are
+        re-recorded when it does."""
+        return int(self._lib.aco_b200_graph_generation(self._h))
 
     def shard_construct(self, d_send: int) -> None:
         """Enqueues weights, construction and the packet of this device's best

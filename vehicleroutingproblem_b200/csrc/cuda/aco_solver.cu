@@ -106,6 +106,7 @@ struct aco_b200_ctx {
 
   cudaGraphExec_t graph_chunk = nullptr;
   cudaGraphExec_t graph_one = nullptr;
+  int graph_gen = 1;  // changes whenever the captured launch arguments may have
   bool run_limit_off = false;  // device run limit known to be disabled
   int depot_rule = 0;
   int inject_alloc = 0;  // test hook: the n-th device allocation of a set-up fails
@@ -141,6 +142,7 @@ void aco_b200_ctx::free_buffers() {
   if (graph_chunk) cudaGraphExecDestroy(graph_chunk);
   if (graph_one) cudaGraphExecDestroy(graph_one);
   graph_chunk = graph_one = nullptr;
+  ++graph_gen;
   void *ptrs[] = {d_coords, d_demand, d_cand, d_lvl, d_thr, d_A, d_lut, d_tau, d_tau2,
                   d_w, d_rel, ab.routes, ab.lens, ab.cost, ab.feasible, ab.steps,
                   ab.draws, ab.loads, ab.rep, ab.repc, d_state, d_log,
@@ -517,6 +519,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
     if (ctx->graph_one) cudaGraphExecDestroy(ctx->graph_one);
     ctx->graph_chunk = ctx->graph_one = nullptr;
     memcpy(ctx->graph_key, key, sizeof(key));
+    ++ctx->graph_gen;
   }
   ctx->ready = true;
   return ACO_OK;
@@ -628,6 +631,7 @@ int aco_b200_debug_inject(aco_b200_ctx *ctx, int what, int value) {
     if (ctx->graph_one) cudaGraphExecDestroy(ctx->graph_one);
     ctx->graph_chunk = ctx->graph_one = nullptr;
     memset(ctx->graph_key, 0, sizeof(ctx->graph_key));
+    ++ctx->graph_gen;
     return ACO_OK;
   }
   return ACO_ERR_INVALID_INPUT;
@@ -664,6 +668,11 @@ int aco_b200_apply_prior_mode(aco_b200_ctx *ctx, aco_b200_prior *prior, float ga
 
 int aco_b200_apply_prior(aco_b200_ctx *ctx, aco_b200_prior *prior, float gamma) {
   return aco_b200_apply_prior_mode(ctx, prior, gamma, 0);
+}
+
+int aco_b200_graph_generation(aco_b200_ctx *ctx) {
+  if (!ctx || !ctx->ready) return -1;
+  return ctx->graph_gen & 0x7fffffff;
 }
 
 int aco_b200_shard_packet_ints(aco_b200_ctx *ctx) {

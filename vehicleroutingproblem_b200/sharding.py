@@ -113,9 +113,19 @@ class ShardedColony:
     Each rank holds an aco_b200 context on its GPU with `ants` ants and
     ant_base = rank * ants; work is queued on one CUDA stream, the packet
     all-gather included, so an epoch costs the host no synchronisation.
+    Over NCCL (graphs=True, the default there) whole epochs, the all-gather
+    included, are recorded once into CUDA graphs of 1 and `chunk` epochs
+    and replayed, so an epoch is one graph launch instead of five kernel
+    launches, two event waits and a collective call; the graphs are
+    re-recorded when a set-up changes the launch arguments
+    (Context.graph_generation) and released by close(), which must come
+    before the process group is destroyed.
     """
 
-    def __init__(self, inst, ants: int, device: int, group=None, stream=None, **params):
+    CHUNK = 16
+
+    def __init__(self, inst, ants: int, device: int, group=None, stream=None,
+                 graphs: Optional[bool] = None, **params):
         import torch
         import torch.distributed as dist
         self.group = group
@@ -124,6 +134,11 @@ class ShardedColony:
         self.device = torch.device("cuda", device)
         self.stream = stream if stream is not None else torch.cuda.Stream(self.device)
         self.ants = ants
+        if graphs is None:
+            graphs = dist.get_backend(group) == "nccl"
+        self.use_graphs = bool(graphs)
+        self._graphs = {}
+        self._warm = False  # one eager epoch since construction (NCCL set up)
         self.ctx = N.Context(device)
         self.ctx.set_stream(self.stream.cuda_stream)
         self.send = self.recv = None
@@ -144,18 +159,47 @@ class ShardedColony:
         self._t0 = time.monotonic()
 
     def close(self) -> None:
+        self._graphs.clear()
         self.ctx.close()
 
-    def enqueue_epoch(self) -> None:
+    def _enqueue_eager(self, epochs: int) -> None:
         import torch
         with torch.cuda.stream(self.stream):
-            self.ctx.shard_construct(self.send.data_ptr())
-            exchange(self.send, self.recv, self.group)
-            self.ctx.shard_update(self.recv.data_ptr(), self.world)
+            for _ in range(epochs):
+                self.ctx.shard_construct(self.send.data_ptr())
+                exchange(self.send, self.recv, self.group)
+                self.ctx.shard_update(self.recv.data_ptr(), self.world)
+
+    def _graph(self, epochs: int):
+        """The recorded graph of `epochs` epochs for the current launch
+        arguments (recorded on first use)."""
+        import torch
+        key = (self.ctx.graph_generation(), self.send.data_ptr(), self.recv.data_ptr(), epochs)
+        g = self._graphs.get(key)
+        if g is None:
+            self._graphs = {k: v for k, v in self._graphs.items() if k[:3] == key[:3]}
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=self.stream, capture_error_mode="thread_local"):
+                self._enqueue_eager(epochs)
+            self._graphs[key] = g
+        return g
 
     def enqueue_epochs(self, epochs: int) -> None:
-        for _ in range(epochs):
-            self.enqueue_epoch()
+        import torch
+        if not self.use_graphs or not self._warm:
+            if epochs > 0:
+                self._enqueue_eager(1)
+                self._warm = True
+                self.enqueue_epochs(epochs - 1)
+            return
+        with torch.cuda.stream(self.stream):
+            for _ in range(epochs // self.CHUNK):
+                self._graph(self.CHUNK).replay()
+            for _ in range(epochs % self.CHUNK):
+                self._graph(1).replay()
+
+    def enqueue_epoch(self) -> None:
+        self.enqueue_epochs(1)
 
     def run(self, max_epochs: int, chunk: int = 16) -> N.State:
         """Runs up to max_epochs epochs, stopping on the device stop rules

@@ -905,7 +905,9 @@ def batched_h2d_d2h(insts):
 
 def run_batched(args, rank, world, local, torch, dist, _native):
     insts_all = I.batched_instances(BATCHED["count"], BATCHED["seed0"])
-    mine = list(range(rank, len(insts_all), world))  # this rank's slice
+    from vehicleroutingproblem_b200 import sharding as S
+    # this rank's share, balanced by the ant-steps per epoch, m (n + K)
+    mine = S.split_instances([x.n + x.vehicles for x in insts_all], world)[rank]
     insts = [insts_all[i] for i in mine]
     r = batched_measure(torch, local, _native, insts, BATCHED["seed0"], args.steps, args.warmup,
                         args.e2e_steps, args.looped_sample if rank == 0 else 0, dist, world)

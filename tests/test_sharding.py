@@ -202,3 +202,20 @@ def test_lost_rank_is_reported_not_waited_for(tmp_path):
     outcome, secs = (tmp_path / "rank0.txt").read_text().splitlines()[:2]
     assert outcome.startswith("error"), outcome
     assert float(secs) < 30.0
+
+
+def test_split_instances_balances_work():
+    """The batched form's split over ranks: every instance once, the ranks'
+    work within one instance's work of each other, deterministic."""
+    insts = I.batched_instances(512, 30000)
+    work = [x.n + x.vehicles for x in insts]
+    for world in (1, 2, 3, 8):
+        parts = S.split_instances(work, world)
+        assert len(parts) == world
+        assert sorted(i for p in parts for i in p) == list(range(len(insts)))
+        loads = [sum(work[i] for i in p) for p in parts]
+        assert max(loads) - min(loads) <= max(work)
+        assert parts == S.split_instances(work, world)
+    assert S.split_instances([5, 3, 3, 1], 2) == [[0, 3], [1, 2]]
+    with pytest.raises(ValueError):
+        S.split_instances(work, 0)

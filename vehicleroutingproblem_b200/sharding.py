@@ -92,6 +92,23 @@ def select_winner(packets: Sequence[Packet]) -> Optional[int]:
     return best
 
 
+def split_instances(work: Sequence[float], world: int) -> List[List[int]]:
+    """The batched form over `world` GPUs: instance indices per rank, the
+    instances being independent (no collective, only the results are
+    gathered).  Largest work first to the rank with the least work so far
+    (ties to the lower rank); each rank's list in ascending order.  The work
+    of an instance is m (n + K) ant-steps per epoch, so with equal m, n + K."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    loads = [0.0] * world
+    parts: List[List[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(work)), key=lambda j: (-float(work[j]), j)):
+        r = min(range(world), key=lambda q: (loads[q], q))
+        parts[r].append(i)
+        loads[r] += float(work[i])
+    return [sorted(p) for p in parts]
+
+
 def exchange(send, recv, group=None) -> None:
     """All-gather of the packets in rank order: send (P words) -> recv
     (world * P words), torch tensors on the process group's device."""

@@ -403,6 +403,62 @@ struct Visited {
   }
 };
 
+// The full scan over a bitmap in shared memory (word wi holds nodes 32 wi ..
+// 32 wi + 31): lane L walks words L, L + 32, ... in ascending node order.
+// Its unvisited nodes are taken kScanBatch at a time and their coordinate
+// (and demand) loads issued together, so a lane waits once per batch rather
+// than once per node; they are still compared in ascending order, so the
+// lane's first nearest node wins.  Returns the lane's best node (its
+// squared distance's bits in *best_h_out).  Out of line: the batch's
+// registers do not weigh on the step loop that calls it (the scan is rare).
+template <int L, bool UNIT>
+__device__ __noinline__ uint32_t scan_words(const float2 *coords, const int *dem,
+                                            const uint32_t *s, int vw, float2 pc, int room,
+                                            bool check_dem, int lane, uint32_t *best_h_out) {
+  uint32_t best_h = 0xffffffffu, best_n = 0xffffffffu;
+  auto visit = [&](int node, float2 p, int dm) {
+    if (!UNIT && check_dem && dm > room) return;
+    const uint32_t h = __float_as_uint(dist2f(pc, p));
+    if (h < best_h) {
+      best_h = h;
+      best_n = (uint32_t)node;
+    }
+  };
+  constexpr int kScanBatch = 16;
+  const int nwords = lane < vw ? (vw - 1 - lane) / 32 + 1 : 0;
+  int j = 0;
+  uint32_t fr = nwords > 0 ? ~s[lane] : 0u;
+  while (true) {
+    int nd[kScanBatch];
+#pragma unroll
+    for (int q = 0; q < kScanBatch; ++q) {
+      while (fr == 0u && ++j < nwords) fr = ~s[lane + 32 * j];
+      nd[q] = -1;
+      if (fr) {
+        nd[q] = ((lane + 32 * j) << 5) + __ffs(fr) - 1;
+        fr &= fr - 1;
+      }
+    }
+    float2 pq[kScanBatch];
+    int dq[kScanBatch];
+#pragma unroll
+    for (int q = 0; q < kScanBatch; ++q) {
+      pq[q] = make_float2(0.f, 0.f);
+      dq[q] = 0;
+      if (nd[q] >= 0) {
+        pq[q] = L == kLayoutGlobal ? __ldg(coords + nd[q]) : coords[nd[q]];
+        if (!UNIT && check_dem) dq[q] = L == kLayoutGlobal ? __ldg(dem + nd[q]) : dem[nd[q]];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kScanBatch; ++q)
+      if (nd[q] >= 0) visit(nd[q], pq[q], dq[q]);
+    if (nd[kScanBatch - 1] < 0) break;
+  }
+  *best_h_out = best_h;
+  return best_n;
+}
+
 // Nearest unvisited customer that fits (find_nearest_unvisited,
 // src/seq/aco_sequential.c:477-493: strict '<' over ascending nodes, so the
 // lowest index wins ties).  0 if none.
@@ -435,41 +491,8 @@ __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
     scan(~vis.w0, lane);
     if (V == 2) scan(~vis.w1, 1024 + lane);
   } else {
-    // Words wi = lane + 32 j of the bitmap, bit b node 32 wi + b.  The
-    // unvisited nodes are taken kScanBatch at a time and their coordinate
-    // (and demand) loads issued together, so a lane waits once per batch
-    // rather than once per node; they are still compared in ascending order.
-    constexpr int kScanBatch = 16;
-    const int nwords = lane < vis.vw ? (vis.vw - 1 - lane) / 32 + 1 : 0;
-    int j = 0;
-    uint32_t fr = nwords > 0 ? ~vis.s[lane] : 0u;
-    while (true) {
-      int nd[kScanBatch];
-#pragma unroll
-      for (int q = 0; q < kScanBatch; ++q) {
-        while (fr == 0u && ++j < nwords) fr = ~vis.s[lane + 32 * j];
-        nd[q] = -1;
-        if (fr) {
-          nd[q] = ((lane + 32 * j) << 5) + __ffs(fr) - 1;
-          fr &= fr - 1;
-        }
-      }
-      float2 pq[kScanBatch];
-      int dq[kScanBatch];
-#pragma unroll
-      for (int q = 0; q < kScanBatch; ++q) {
-        pq[q] = make_float2(0.f, 0.f);
-        dq[q] = 0;
-        if (nd[q] >= 0) {
-          pq[q] = tb.coord(nd[q]);
-          if (!UNIT && check_dem) dq[q] = tb.demand(nd[q]);
-        }
-      }
-#pragma unroll
-      for (int q = 0; q < kScanBatch; ++q)
-        if (nd[q] >= 0) visit(nd[q], pq[q], dq[q]);
-      if (nd[kScanBatch - 1] < 0) break;
-    }
+    best_n = scan_words<L, UNIT>(tb.coords, tb.dem, vis.s, vis.vw, pc, room, check_dem, lane,
+                                 &best_h);
   }
   const uint32_t mh = __reduce_min_sync(kFull, best_h);
   const uint32_t mn = __reduce_min_sync(kFull, best_h == mh ? best_n : 0xffffffffu);

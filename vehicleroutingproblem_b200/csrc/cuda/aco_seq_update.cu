@@ -15,12 +15,16 @@
 //   k_seq_sweep    the matrix two cells (16 bytes) at a time, four pairs per
 //                  thread in flight: evaporate; unmarked cells also clamp
 //                  and reset
-//   k_seq_deposit  one block: the iteration-best adds, then the global-best
-//                  adds (double atomics: the adds to one cell within one
-//                  deposit are of the same amount, so their order does not
-//                  change the sum), then every marked cell is clamped and
-//                  reset by the thread that clears its bit -- which leaves the
-//                  bitmap zeroed for the next call.
+//   k_seq_add      the adds of one solution, one launch for the iteration
+//                  best, then one for the global best (double atomics: the
+//                  adds to one cell within one deposit are of the same
+//                  amount, so their order does not change the sum; the
+//                  launch boundary orders the two deposits)
+//   k_seq_clamp    every marked cell clamped and reset by the thread that
+//                  clears its bit -- which leaves the bitmap zeroed for the
+//                  next call.
+// The arc kernels deal a solution's arcs over all their threads, one arc
+// per thread at the sizes of interest (n + K arcs).
 // Every operation is an IEEE FP64 multiply, add or compare in the
 // reference's order, written with __dmul_rn/__dadd_rn so that nothing is
 // contracted into a fused multiply-add.
@@ -96,14 +100,17 @@ __device__ __forceinline__ unsigned long long cell(int n, int u, int v) {
   return (unsigned long long)u * (unsigned long long)(n + 1) + (unsigned long long)v;
 }
 
-__global__ void __launch_bounds__(1024) k_seq_mark(SeqArgs a) {
+constexpr int kArcThreads = 256;
+
+__global__ void __launch_bounds__(kArcThreads) k_seq_mark(SeqArgs a) {
   extern __shared__ int s_off[];
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
   for (int which = 0; which < 2; ++which) {
     const int *nodes = which ? a.gb_nodes : a.it_nodes;
     const int *lens = which ? a.gb_lens : a.it_lens;
     if (!nodes) break;
     const int total = load_arc_offsets(lens, a.K, s_off);
-    for (int j = threadIdx.x; j < total; j += blockDim.x) {
+    for (int j = gt; j < total; j += gn) {
       int u, v;
       arc_of(nodes, s_off, a.K, j, &u, &v);
       if (u == v) continue;  // the diagonal is never swept
@@ -175,31 +182,33 @@ __global__ void __launch_bounds__(kSweepThreads) k_seq_sweep(SeqArgs a) {
   // on the diagonal, which the update never changes.
 }
 
-__global__ void __launch_bounds__(1024) k_seq_deposit(SeqArgs a) {
+// The adds of one solution (which = 0: the iteration best, 1: the global
+// best) into the evaporated matrix.
+__global__ void __launch_bounds__(kArcThreads) k_seq_add(SeqArgs a, int which) {
   extern __shared__ int s_off[];
-  for (int which = 0; which < 2; ++which) {
-    const int *nodes = which ? a.gb_nodes : a.it_nodes;
-    const int *lens = which ? a.gb_lens : a.it_lens;
-    if (!nodes) break;
-    const double d = which ? a.d_gb : a.d_it;
-    const int total = load_arc_offsets(lens, a.K, s_off);
-    for (int j = threadIdx.x; j < total; j += blockDim.x) {
-      int u, v;
-      arc_of(nodes, s_off, a.K, j, &u, &v);
-      atomicAdd(a.tau + cell(a.n, u, v), d);
-      atomicAdd(a.tau + cell(a.n, v, u), d);
-    }
-    // every add of this deposit before any of the next (or the clamps)
-    __threadfence();
-    __syncthreads();
+  const int *nodes = which ? a.gb_nodes : a.it_nodes;
+  const int *lens = which ? a.gb_lens : a.it_lens;
+  const double d = which ? a.d_gb : a.d_it;
+  const int total = load_arc_offsets(lens, a.K, s_off);
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
+  for (int j = gt; j < total; j += gn) {
+    int u, v;
+    arc_of(nodes, s_off, a.K, j, &u, &v);
+    atomicAdd(a.tau + cell(a.n, u, v), d);
+    atomicAdd(a.tau + cell(a.n, v, u), d);
   }
-  // Clamp and reset each marked cell once: the thread that clears its bit.
+}
+
+// Clamp and reset each marked cell once: the thread that clears its bit.
+__global__ void __launch_bounds__(kArcThreads) k_seq_clamp(SeqArgs a) {
+  extern __shared__ int s_off[];
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
   for (int which = 0; which < 2; ++which) {
     const int *nodes = which ? a.gb_nodes : a.it_nodes;
     const int *lens = which ? a.gb_lens : a.it_lens;
     if (!nodes) break;
     const int total = load_arc_offsets(lens, a.K, s_off);
-    for (int j = threadIdx.x; j < total; j += blockDim.x) {
+    for (int j = gt; j < total; j += gn) {
       int u, v;
       arc_of(nodes, s_off, a.K, j, &u, &v);
       if (u == v) continue;
@@ -267,9 +276,16 @@ extern "C" ACO_API int aco_b200_seq_pheromone_update(
   if (g > (unsigned long long)sms * 8) g = (unsigned long long)sms * 8;
   if (g < 1) g = 1;
   const int grid = (int)g;
-  k_seq_mark<<<1, 1024, smem, s>>>(a);
+  // The arc kernels: enough blocks for one arc per thread (a solution has
+  // n + K arcs at most), at most 4 per SM.
+  unsigned long long ga = ((unsigned long long)n + K + kArcThreads - 1) / kArcThreads;
+  if (ga > (unsigned long long)sms * 4) ga = (unsigned long long)sms * 4;
+  const int arc_grid = (int)ga;
+  k_seq_mark<<<arc_grid, kArcThreads, smem, s>>>(a);
   k_seq_sweep<<<grid, kSweepThreads, 0, s>>>(a);
-  k_seq_deposit<<<1, 1024, smem, s>>>(a);
+  k_seq_add<<<arc_grid, kArcThreads, smem, s>>>(a, 0);
+  if (a.gb_nodes) k_seq_add<<<arc_grid, kArcThreads, smem, s>>>(a, 1);
+  k_seq_clamp<<<arc_grid, kArcThreads, smem, s>>>(a);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     fprintf(stderr, "aco_b200_seq_pheromone_update: %s\n", cudaGetErrorString(e));

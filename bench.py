@@ -498,7 +498,8 @@ def update_roofline(ctx, n, launches, peak, peak_kind):
     """Roofline of the pheromone evaporation sweep (k_evaporate_to, the
     reference's kernel_evaporate_tau) on this context's matrix: 2 (n+1)^2
     algorithmic bytes (each byte read once and written once) per launch over
-    the mean CUDA-event time of one launch, the sweep timed alone."""
+    the device time of one launch, the sweep timed alone: `launches`
+    launches back to back between two CUDA events (after one untimed)."""
     ms = ctx.profile_update(launches)
     nbytes = 2 * (n + 1) ** 2
     achieved = nbytes / (ms / 1e3) / 1e9
@@ -506,6 +507,7 @@ def update_roofline(ctx, n, launches, peak, peak_kind):
     return {"bound": "hbm", "kernel": "k_evaporate_to", "achieved": achieved, "peak": peak,
             "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind, "n": n,
             "bytes_per_launch": nbytes, "us_per_launch": ms * 1e3, "launches": launches,
+            "timing": "launches back to back between two CUDA events on the sweep's stream",
             "residency": ("L2-resident: both matrices fit in L2, so this is not an HBM figure"
                           if resident else "HBM: the matrices exceed L2"),
             "traffic": UPDATE_DRAM_BYTES_PER_LAUNCH.get(n),

@@ -121,8 +121,9 @@ ACO_API int aco_b200_profile_epochs(aco_b200_ctx *ctx, int epochs, float *kernel
  * kernel and grid the epoch graph uses (current buffer into the other one,
  * which the next epoch overwrites; the current buffer and the solve's
  * progress are left unchanged, and the run limit is cleared as by
- * aco_b200_enqueue_epochs), each between two CUDA events on the context
- * stream.  *ms_per_launch is the mean device time of one launch.  The sweep
+ * aco_b200_enqueue_epochs): one untimed launch, then `launches` launches
+ * back to back between two CUDA events on the context stream.
+ * *ms_per_launch is the events' interval over `launches`.  The sweep
  * moves 2 (n+1)^2 bytes (read + write); the reference's counterpart is
  * kernel_evaporate_tau (src/cuda/aco_cuda_kernels.cu:145-155). */
 ACO_API int aco_b200_profile_update(aco_b200_ctx *ctx, int launches, float *ms_per_launch);

@@ -114,6 +114,19 @@ def test_fallback_tier_lists(oracle_mod, name):
         assert np.array_equal(ctx.tier().reshape(inst.n + 1, 64), full[:, kk:].astype(np.uint16))
 
 
+def test_fallback_second_tier_lists(oracle_mod):
+    """The second tier of a large instance (n >= 4000): ranks k+65 .. k+256
+    of the oracle's nearest-neighbour order; smaller instances have none."""
+    inst = I.uniform_instance(4500, 12, 7801)
+    with make_ctx(inst, 32, 8) as ctx:
+        full = oracle_mod.knn(inst.x, inst.y, 32 + 256).reshape(inst.n + 1, 32 + 256)
+        assert np.array_equal(ctx.tier().reshape(inst.n + 1, 64), full[:, 32:96].astype(np.uint16))
+        assert np.array_equal(ctx.tier2().reshape(inst.n + 1, 192), full[:, 96:].astype(np.uint16))
+    with make_ctx(CASES["u3000_demand"][0](), 32, 8) as ctx:
+        with pytest.raises(_native.AcoError):
+            ctx.tier2()
+
+
 @pytest.mark.parametrize("name", ["u200_unit", "u300_demand", "n1000_c2"])
 @pytest.mark.parametrize("mode", ["random", "mostly_init"])
 def test_weights(oracle_mod, name, mode):

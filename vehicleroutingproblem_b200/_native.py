@@ -30,6 +30,7 @@ EXPORTED = [
     "aco_b200_run", "aco_b200_enqueue_epochs", "aco_b200_synchronize",
     "aco_b200_get_best", "aco_b200_get_state", "aco_b200_get_dims", "aco_b200_get_plan",
     "aco_b200_get_tau", "aco_b200_set_tau", "aco_b200_get_candidates", "aco_b200_get_tier",
+    "aco_b200_get_tier2",
     "aco_b200_get_tables", "aco_b200_get_weights", "aco_b200_construct",
     "aco_b200_get_ants", "aco_b200_evaporate_deposit", "aco_b200_build_info",
     "aco_b200_profile_epochs", "aco_b200_profile_update", "aco_b200_evaporate_deposit_noalloc",
@@ -124,6 +125,7 @@ def load():
         "aco_b200_get_dims": [vp, vp, vp, vp, vp], "aco_b200_get_plan": [vp, vp],
         "aco_b200_get_tau": [vp, vp], "aco_b200_set_tau": [vp, vp],
         "aco_b200_get_candidates": [vp, vp, vp], "aco_b200_get_tier": [vp, vp],
+        "aco_b200_get_tier2": [vp, vp],
         "aco_b200_get_tables": [vp, vp, vp, vp, i32],
         "aco_b200_get_weights": [vp, vp], "aco_b200_construct": [vp, i32, i32],
         "aco_b200_get_ants": [vp, vp, vp, vp, vp, vp, vp],
@@ -324,6 +326,12 @@ class Context:
         """Neighbours of ranks k+1 .. k+64 of every node ([(n+1) 64], 0 = empty)."""
         t = np.zeros((self.n + 1) * 64, np.uint16)
         _check(self._lib.aco_b200_get_tier(self._h, _p(t)), "aco_b200_get_tier")
+        return t
+
+    def tier2(self) -> np.ndarray:
+        """Neighbours of ranks k+65 .. k+256 ([(n+1) 192], 0 = empty; n >= 4000)."""
+        t = np.zeros((self.n + 1) * 192, np.uint16)
+        _check(self._lib.aco_b200_get_tier2(self._h, _p(t)), "aco_b200_get_tier2")
         return t
 
     def tables(self):

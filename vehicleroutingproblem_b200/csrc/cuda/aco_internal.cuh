@@ -123,11 +123,17 @@ struct InstanceView {
   // ([(n+1) kTierLen], 0 = none), or null: the nearest-customer fallback
   // looks there before it scans every node.
   const uint16_t *tier;
+  // Ranks k+65 .. k+64+kTier2Len ([(n+1) kTier2Len], 0 = none), or null:
+  // looked at after the tier lists, before the scan (large instances).
+  const uint16_t *tier2;
 };
 
 constexpr int kTierLen = 64;
 // Smallest instance whose construction uses the tier lists.
 constexpr int kTierMinCustomers = 512;
+constexpr int kTier2Len = 192;
+// Smallest instance whose construction uses the second tier lists.
+constexpr int kTier2MinCustomers = 4000;
 
 struct AntBuffers {
   int *routes;             // [m][n + 2K] compact routes
@@ -167,7 +173,8 @@ struct PheromoneView {
 cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
                               const float *thr, int J, uint16_t *cand,
                               uint16_t *lvl, cudaStream_t s);
-cudaError_t launch_knn_tier(const float2 *coords, int n, int k, uint16_t *tier, cudaStream_t s);
+cudaError_t launch_knn_tier(const float2 *coords, int n, int k, uint16_t *tier, uint16_t *tier2,
+                            cudaStream_t s);
 cudaError_t launch_knn_tier_multi(const float2 *coords, const long long *seg_off,
                                   const int *seg_n, int count, long long rows, int k,
                                   uint16_t *tier, cudaStream_t s);

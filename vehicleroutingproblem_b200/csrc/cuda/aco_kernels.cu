@@ -73,7 +73,8 @@ cudaError_t launch_knn_levels(const float2 *coords, int n, int k,
 // node).  0 marks an empty slot; an empty last slot means the candidates and
 // this row hold every other customer.
 __global__ void __launch_bounds__(256) k_knn_tier(const float2 *__restrict__ coords, int n,
-                                                  int k, uint16_t *__restrict__ tier) {
+                                                  int k, uint16_t *__restrict__ tier,
+                                                  uint16_t *__restrict__ tier2) {
   const int lane = threadIdx.x & 31;
   const int warps = gridDim.x * (blockDim.x >> 5);
   const unsigned long long kNone = ~0ull;
@@ -88,14 +89,24 @@ __global__ void __launch_bounds__(256) k_knn_tier(const float2 *__restrict__ coo
       last_lane = 31;
       row[32 * r + lane] = (uint16_t)(key == kNone ? 0u : (unsigned)(key & 0xffffffffu));
     }
+    if (!tier2) continue;
+    // The second tier: the next kTier2Len ranks, 32 per pass as above.
+    uint16_t *row2 = tier2 + (size_t)i * kTier2Len;
+#pragma unroll 1
+    for (int r = 0; r < kTier2Len / 32; ++r) {
+      const unsigned long long last = __shfl_sync(kFull, key, 31);
+      key = (last == kNone) ? kNone : warp_knn(coords, n, 32, i, lane, last);
+      row2[32 * r + lane] = (uint16_t)(key == kNone ? 0u : (unsigned)(key & 0xffffffffu));
+    }
   }
 }
 
-cudaError_t launch_knn_tier(const float2 *coords, int n, int k, uint16_t *tier, cudaStream_t s) {
+cudaError_t launch_knn_tier(const float2 *coords, int n, int k, uint16_t *tier, uint16_t *tier2,
+                            cudaStream_t s) {
   if (k < 1 || k > kMaxCand) return cudaErrorInvalidValue;
   int blocks = (n + 1 + 7) / 8;
   if (blocks > 148 * 16) blocks = 148 * 16;
-  k_knn_tier<<<blocks, 256, 0, s>>>(coords, n, k, tier);
+  k_knn_tier<<<blocks, 256, 0, s>>>(coords, n, k, tier, tier2);
   return cudaGetLastError();
 }
 
@@ -312,6 +323,7 @@ __device__ __forceinline__ void draw_refill(uint32_t *buf, uint32_t d,
 template <int L, bool UNIT>
 struct Tables {
   const uint16_t *tier;  // global, or null
+  const uint16_t *tier2;  // global, or null
   const uint16_t *cand;
   const uint32_t *w;
   const uint8_t *rel;
@@ -499,6 +511,34 @@ __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
   return (mh == 0xffffffffu) ? 0 : (int)mn;
 }
 
+// The first eligible node of a second-tier row (the bitmap in shared memory,
+// word wi holding nodes 32 wi .. 32 wi + 31): the node (> 0); 0 when the row
+// lists every remaining customer and none is eligible; -1 when none of the
+// row is eligible and the row is full (customers beyond it remain).  All of
+// the row and its demands are loaded at once.  Out of line: it is rare.
+template <int L, bool UNIT>
+__device__ __noinline__ int tier2_first(const uint16_t *row, const uint32_t *s, const int *dem,
+                                        int room, bool check_dem, int lane) {
+  constexpr int kParts = kTier2Len / 32;
+  int nodes[kParts], dq[kParts];
+#pragma unroll
+  for (int r = 0; r < kParts; ++r) nodes[r] = (int)__ldg(row + 32 * r + lane);
+#pragma unroll
+  for (int r = 0; r < kParts; ++r)
+    dq[r] = (!UNIT && check_dem) ? (L == kLayoutGlobal ? __ldg(dem + nodes[r]) : dem[nodes[r]]) : 0;
+#pragma unroll
+  for (int r = 0; r < kParts; ++r) {
+    const int node = nodes[r];
+    const uint32_t word = s[node >> 5];
+    // node 0 (empty slot) reads as visited: the depot's bit is set
+    bool ok = ((__funnelshift_r(word, word, node) & 1u) == 0u);
+    if (!UNIT && check_dem) ok = ok && dq[r] <= room;
+    const unsigned m = __ballot_sync(kFull, ok);
+    if (m) return __shfl_sync(kFull, node, __ffs(m) - 1);
+  }
+  return (__shfl_sync(kFull, nodes[kParts - 1], 31) == 0) ? 0 : -1;
+}
+
 // Nearest eligible customer of the fallback, when no candidate of row cur
 // has a weight (find_nearest_unvisited's rule, as nearest_unvisited): the
 // first eligible candidate (okm: the row's eligible candidates; they come
@@ -526,6 +566,11 @@ __device__ __forceinline__ int nearest_eligible(const Tables<L, UNIT> &tb, const
     }
     // every customer was listed
     if (__shfl_sync(kFull, nodes[kTierLen / 32 - 1], 31) == 0) return 0;
+    if (V == 0 && tb.tier2) {
+      const int r = tier2_first<L, UNIT>(tb.tier2 + (size_t)cur * kTier2Len, vis.s, tb.dem, room,
+                                         check_dem, lane);
+      if (r >= 0) return r;
+    }
   }
   return nearest_unvisited<L, UNIT, V>(tb, vis, tb.coord(cur), room, check_dem, lane);
 }
@@ -845,6 +890,7 @@ __global__ void __launch_bounds__(512, 1) k_construct(ConstructArgs a) {
 
   Tables<L, UNIT> tb;
   tb.tier = iv.tier;
+  tb.tier2 = iv.tier2;
   if (L == kLayoutGlobal) {
     tb.cand = iv.cand;
     tb.w = a.et.w;

@@ -77,6 +77,7 @@ struct aco_b200_ctx {
   int *d_demand = nullptr;
   uint16_t *d_cand = nullptr, *d_lvl = nullptr;
   uint16_t *d_tier = nullptr;  // neighbours of ranks k+1 .. k+64 (fallback)
+  uint16_t *d_tier2 = nullptr;  // ranks k+65 .. k+256 (fallback, n >= kTier2MinCustomers)
   float *d_thr = nullptr;
   int32_t *d_A = nullptr;
   uint32_t *d_lut = nullptr;
@@ -147,7 +148,7 @@ void aco_b200_ctx::free_buffers() {
                   d_w, d_rel, ab.routes, ab.lens, ab.cost, ab.feasible, ab.steps,
                   ab.draws, ab.loads, ab.rep, ab.repc, d_state, d_log,
                   d_gbest_nodes, d_gbest_lens, d_tmp_nodes, d_tmp_lens, d_iter_nodes,
-                  d_iter_lens, d_counter, d_rdep, d_lvl0, d_tier};
+                  d_iter_lens, d_counter, d_rdep, d_lvl0, d_tier, d_tier2};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   d_coords = nullptr; d_demand = nullptr; d_cand = d_lvl = nullptr; d_thr = nullptr;
@@ -156,7 +157,7 @@ void aco_b200_ctx::free_buffers() {
   ab = AntBuffers{};
   d_state = nullptr; d_log = nullptr; d_gbest_nodes = d_gbest_lens = nullptr;
   d_tmp_nodes = d_tmp_lens = nullptr; d_iter_nodes = d_iter_lens = nullptr;
-  d_rdep = nullptr; d_lvl0 = nullptr; d_tier = nullptr;
+  d_rdep = nullptr; d_lvl0 = nullptr; d_tier = nullptr; d_tier2 = nullptr;
   d_counter = nullptr;
   ready = false;
 }
@@ -403,6 +404,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
     TRY_ALLOC(dalloc(&ctx->d_cand, rows * k));
     TRY_ALLOC(dalloc(&ctx->d_lvl, rows * k));
     TRY_ALLOC(dalloc(&ctx->d_tier, rows * kTierLen));
+    if (n >= kTier2MinCustomers) TRY_ALLOC(dalloc(&ctx->d_tier2, rows * kTier2Len));
     TRY_ALLOC(dalloc(&ctx->d_thr, (size_t)kThresholds));
     TRY_ALLOC(dalloc(&ctx->d_A, 256));
     TRY_ALLOC(dalloc(&ctx->d_lut, 256));
@@ -468,6 +470,9 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   // the full scan is long (each lane walks (n+1)/32 bitmap bits): at n=1000
   // the construction takes 279 -> 268 us with them, at n=100 34.2 -> 36.0.
   iv.tier = (n >= kTierMinCustomers) ? ctx->d_tier : nullptr;
+  // The second tier (ranks k+65 .. k+256) where a full scan walks thousands
+  // of bitmap words.
+  iv.tier2 = (n >= kTier2MinCustomers) ? ctx->d_tier2 : nullptr;
   PheromoneView &pv = ctx->pv;
   pv.tau = ctx->d_tau;
   pv.total = tau_total;
@@ -490,7 +495,7 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   ctx->evap_grid = evap_grid_for(tau_total, ctx->num_sms);
 
   TRY(launch_knn_levels(ctx->d_coords, n, k, ctx->d_thr, kThresholds, ctx->d_cand, ctx->d_lvl, s));
-  TRY(launch_knn_tier(ctx->d_coords, n, k, ctx->d_tier, s));
+  TRY(launch_knn_tier(ctx->d_coords, n, k, ctx->d_tier, iv.tier2 ? ctx->d_tier2 : nullptr, s));
   TRY(launch_fill_u8(ctx->d_tau, tau_total, ctx->q_tau0, s));
   if (ctx->d_lvl0) TRY(launch_depot_levels(ctx->d_coords, n, ctx->d_thr, kThresholds, ctx->d_lvl0, s));
 
@@ -879,6 +884,15 @@ int aco_b200_get_tier(aco_b200_ctx *ctx, uint16_t *tier) {
   cudaSetDevice(ctx->device);
   const size_t cnt = ((size_t)ctx->n + 1) * kTierLen;
   TRY(cudaMemcpyAsync(tier, ctx->d_tier, cnt * 2, cudaMemcpyDeviceToHost, ctx->stream));
+  TRY(cudaStreamSynchronize(ctx->stream));
+  return ACO_OK;
+}
+
+int aco_b200_get_tier2(aco_b200_ctx *ctx, uint16_t *tier2) {
+  if (!ctx || !ctx->ready || !tier2 || !ctx->iv.tier2) return ACO_ERR_INVALID_INPUT;
+  cudaSetDevice(ctx->device);
+  const size_t cnt = ((size_t)ctx->n + 1) * kTier2Len;
+  TRY(cudaMemcpyAsync(tier2, ctx->d_tier2, cnt * 2, cudaMemcpyDeviceToHost, ctx->stream));
   TRY(cudaStreamSynchronize(ctx->stream));
   return ACO_OK;
 }

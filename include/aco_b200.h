@@ -150,7 +150,7 @@ ACO_API int aco_b200_get_candidates(aco_b200_ctx *ctx, int *cand, uint16_t *leve
  * fallback looks before it scans every node. */
 ACO_API int aco_b200_get_tier(aco_b200_ctx *ctx, uint16_t *tier);
 /* Ranks k+65 .. k+256 of every node ([(n+1) 192], 0 = empty slot), where the
- * fallback looks after the ranks above, for instances of n >= 4000;
+ * fallback looks after the ranks above, for instances of n >= 1500;
  * ACO_ERR_INVALID_INPUT for smaller ones. */
 ACO_API int aco_b200_get_tier2(aco_b200_ctx *ctx, uint16_t *tier2);
 ACO_API int aco_b200_get_tables(aco_b200_ctx *ctx, int32_t *A, uint32_t *lut,

@@ -115,14 +115,18 @@ def test_fallback_tier_lists(oracle_mod, name):
 
 
 def test_fallback_second_tier_lists(oracle_mod):
-    """The second tier of a large instance (n >= 4000): ranks k+65 .. k+256
+    """The second tier of a large instance (n >= 1500): ranks k+65 .. k+256
     of the oracle's nearest-neighbour order; smaller instances have none."""
     inst = I.uniform_instance(4500, 12, 7801)
     with make_ctx(inst, 32, 8) as ctx:
         full = oracle_mod.knn(inst.x, inst.y, 32 + 256).reshape(inst.n + 1, 32 + 256)
         assert np.array_equal(ctx.tier().reshape(inst.n + 1, 64), full[:, 32:96].astype(np.uint16))
         assert np.array_equal(ctx.tier2().reshape(inst.n + 1, 192), full[:, 96:].astype(np.uint16))
-    with make_ctx(CASES["u3000_demand"][0](), 32, 8) as ctx:
+    c2 = CASES["c2000_demand"][0]()  # clustered n=2000: the register bitmap of two words
+    with make_ctx(c2, 32, 8) as ctx:
+        full = oracle_mod.knn(c2.x, c2.y, 32 + 256).reshape(c2.n + 1, 32 + 256)
+        assert np.array_equal(ctx.tier2().reshape(c2.n + 1, 192), full[:, 96:].astype(np.uint16))
+    with make_ctx(CASES["n1000_c2"][0](), 32, 8) as ctx:
         with pytest.raises(_native.AcoError):
             ctx.tier2()
 

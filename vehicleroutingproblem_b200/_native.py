@@ -329,7 +329,7 @@ class Context:
         return t
 
     def tier2(self) -> np.ndarray:
-        """Neighbours of ranks k+65 .. k+256 ([(n+1) 192], 0 = empty; n >= 4000)."""
+        """Neighbours of ranks k+65 .. k+256 ([(n+1) 192], 0 = empty; n >= 1500)."""
         t = np.zeros((self.n + 1) * 192, np.uint16)
         _check(self._lib.aco_b200_get_tier2(self._h, _p(t)), "aco_b200_get_tier2")
         return t

@@ -133,7 +133,7 @@ constexpr int kTierLen = 64;
 constexpr int kTierMinCustomers = 512;
 constexpr int kTier2Len = 192;
 // Smallest instance whose construction uses the second tier lists.
-constexpr int kTier2MinCustomers = 4000;
+constexpr int kTier2MinCustomers = 1500;
 
 struct AntBuffers {
   int *routes;             // [m][n + 2K] compact routes

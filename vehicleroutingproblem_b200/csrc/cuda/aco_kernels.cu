@@ -415,6 +415,57 @@ struct Visited {
   }
 };
 
+// The full scan over a register bitmap of two words per lane (V = 2, the
+// transposed layout of Visited<2>: bit b of word j is node 1024 j + lane +
+// 32 b), in ascending node order, 8 unvisited nodes at a time with their
+// coordinate (and demand) loads issued together; the lane's best node (its
+// squared distance's bits in *best_h_out).  Out of line, as scan_words.
+// (With one word per lane the plain loop is as fast and shorter.)
+template <int L, bool UNIT, int V>
+__device__ __noinline__ uint32_t scan_regs(const float2 *coords, const int *dem, uint32_t w0,
+                                           uint32_t w1, float2 pc, int room, bool check_dem,
+                                           int lane, uint32_t *best_h_out) {
+  uint32_t best_h = 0xffffffffu, best_n = 0xffffffffu;
+  constexpr int kB = 8;
+  int j = 0;
+  uint32_t fr = ~w0;
+  while (true) {
+    int nd[kB];
+#pragma unroll
+    for (int q = 0; q < kB; ++q) {
+      if (V == 2 && fr == 0u && j == 0) { fr = ~w1; j = 1; }
+      nd[q] = -1;
+      if (fr) {
+        nd[q] = 1024 * j + lane + 32 * (__ffs(fr) - 1);
+        fr &= fr - 1;
+      }
+    }
+    float2 pq[kB];
+    int dq[kB];
+#pragma unroll
+    for (int q = 0; q < kB; ++q) {
+      pq[q] = make_float2(0.f, 0.f);
+      dq[q] = 0;
+      if (nd[q] >= 0) {
+        pq[q] = L == kLayoutGlobal ? __ldg(coords + nd[q]) : coords[nd[q]];
+        if (!UNIT && check_dem) dq[q] = L == kLayoutGlobal ? __ldg(dem + nd[q]) : dem[nd[q]];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kB; ++q) {
+      if (nd[q] < 0 || (!UNIT && check_dem && dq[q] > room)) continue;
+      const uint32_t h = __float_as_uint(dist2f(pc, pq[q]));
+      if (h < best_h) {
+        best_h = h;
+        best_n = (uint32_t)nd[q];
+      }
+    }
+    if (nd[kB - 1] < 0) break;
+  }
+  *best_h_out = best_h;
+  return best_n;
+}
+
 // The full scan over a bitmap in shared memory (word wi holds nodes 32 wi ..
 // 32 wi + 31): lane L walks words L, L + 32, ... in ascending node order.
 // Its unvisited nodes are taken kScanBatch at a time and their coordinate
@@ -488,9 +539,11 @@ __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
       best_n = (uint32_t)node;
     }
   };
-  if (V >= 1) {
-    // Bit b of register word j is node 1024 j + lane + 32 b (ascending);
-    // the tables are in shared memory, so one node at a time.
+  if (V == 2) {
+    best_n = scan_regs<L, UNIT, V>(tb.coords, tb.dem, vis.w0, vis.w1, pc, room, check_dem, lane,
+                                   &best_h);
+  } else if (V == 1) {
+    // Bit b of w0 is node lane + 32 b (ascending); one node at a time.
     auto scan = [&](uint32_t fr, int first) {
       while (fr) {
         const int b = __ffs(fr) - 1;
@@ -501,7 +554,6 @@ __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
       }
     };
     scan(~vis.w0, lane);
-    if (V == 2) scan(~vis.w1, 1024 + lane);
   } else {
     best_n = scan_words<L, UNIT>(tb.coords, tb.dem, vis.s, vis.vw, pc, room, check_dem, lane,
                                  &best_h);
@@ -511,14 +563,17 @@ __device__ __forceinline__ int nearest_unvisited(const Tables<L, UNIT> &tb,
   return (mh == 0xffffffffu) ? 0 : (int)mn;
 }
 
-// The first eligible node of a second-tier row (the bitmap in shared memory,
-// word wi holding nodes 32 wi .. 32 wi + 31): the node (> 0); 0 when the row
-// lists every remaining customer and none is eligible; -1 when none of the
-// row is eligible and the row is full (customers beyond it remain).  All of
-// the row and its demands are loaded at once.  Out of line: it is rare.
-template <int L, bool UNIT>
-__device__ __noinline__ int tier2_first(const uint16_t *row, const uint32_t *s, const int *dem,
-                                        int room, bool check_dem, int lane) {
+// The first eligible node of a second-tier row: the node (> 0); 0 when the
+// row lists every remaining customer and none is eligible; -1 when none of
+// the row is eligible and the row is full (customers beyond it remain).  The
+// visited bitmap is read as Visited<V> holds it: V = 0 in shared memory at s
+// (word wi holding nodes 32 wi .. 32 wi + 31), V = 1, 2 in the registers w0,
+// w1 of the lanes (transposed).  All of the row and its demands are loaded
+// at once.  Out of line: it is rare.
+template <int L, bool UNIT, int V>
+__device__ __noinline__ int tier2_first(const uint16_t *row, const uint32_t *s, uint32_t w0,
+                                        uint32_t w1, const int *dem, int room, bool check_dem,
+                                        int lane) {
   constexpr int kParts = kTier2Len / 32;
   int nodes[kParts], dq[kParts];
 #pragma unroll
@@ -529,9 +584,20 @@ __device__ __noinline__ int tier2_first(const uint16_t *row, const uint32_t *s, 
 #pragma unroll
   for (int r = 0; r < kParts; ++r) {
     const int node = nodes[r];
-    const uint32_t word = s[node >> 5];
     // node 0 (empty slot) reads as visited: the depot's bit is set
-    bool ok = ((__funnelshift_r(word, word, node) & 1u) == 0u);
+    bool ok;
+    if (V == 0) {
+      const uint32_t word = s[node >> 5];
+      ok = (__funnelshift_r(word, word, node) & 1u) == 0u;
+    } else {
+      const uint32_t bit = __funnelshift_l(0u, 1u, node >> 5);
+      uint32_t word = __shfl_sync(kFull, w0, node);
+      if (V == 2) {
+        const uint32_t hi = __shfl_sync(kFull, w1, node);
+        word = (node >> 10) ? hi : word;
+      }
+      ok = (word & bit) == 0u;
+    }
     if (!UNIT && check_dem) ok = ok && dq[r] <= room;
     const unsigned m = __ballot_sync(kFull, ok);
     if (m) return __shfl_sync(kFull, node, __ffs(m) - 1);
@@ -566,9 +632,9 @@ __device__ __forceinline__ int nearest_eligible(const Tables<L, UNIT> &tb, const
     }
     // every customer was listed
     if (__shfl_sync(kFull, nodes[kTierLen / 32 - 1], 31) == 0) return 0;
-    if (V == 0 && tb.tier2) {
-      const int r = tier2_first<L, UNIT>(tb.tier2 + (size_t)cur * kTier2Len, vis.s, tb.dem, room,
-                                         check_dem, lane);
+    if (tb.tier2) {
+      const int r = tier2_first<L, UNIT, V>(tb.tier2 + (size_t)cur * kTier2Len, vis.s, vis.w0,
+                                            vis.w1, tb.dem, room, check_dem, lane);
       if (r >= 0) return r;
     }
   }

@@ -470,8 +470,10 @@ int aco_b200_setup(aco_b200_ctx *ctx, const aco_b200_problem *p) {
   // the full scan is long (each lane walks (n+1)/32 bitmap bits): at n=1000
   // the construction takes 279 -> 268 us with them, at n=100 34.2 -> 36.0.
   iv.tier = (n >= kTierMinCustomers) ? ctx->d_tier : nullptr;
-  // The second tier (ranks k+65 .. k+256) where a full scan walks thousands
-  // of bitmap words.
+  // The second tier (ranks k+65 .. k+256) from n = 1500 on, where the full
+  // scan walks two or more bitmap words per lane: clustered n=2000 756 ->
+  // 706 us with it, n=3000 1544 -> 1420 us; at n=1000 (one word per lane)
+  // its L2 loads cost more than the scans they replace.
   iv.tier2 = (n >= kTier2MinCustomers) ? ctx->d_tier2 : nullptr;
   PheromoneView &pv = ctx->pv;
   pv.tau = ctx->d_tau;

@@ -103,6 +103,8 @@ struct SmemPlan {
   int vreg;                // bitmap words per lane held in registers (0: smem)
   int wpb;                 // warps (ants) per block
   int layout;
+  uint32_t off_route;      // route_smem: each ant's route (route_stride ints) in shared memory
+  int route_smem;
 };
 
 struct InstanceView {

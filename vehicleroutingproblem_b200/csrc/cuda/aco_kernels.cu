@@ -247,6 +247,20 @@ __global__ void __launch_bounds__(256) k_weights(InstanceView iv,
                                                  PheromoneView pv,
                                                  EpochTables et,
                                                  DevState *st) {
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int k = iv.k;
+  const size_t stride = (size_t)iv.n + 1;
+  // This warp's first row's candidates and levels, the buffer selector and
+  // the stop flag are all requested before any of them is used, so that
+  // their round trips overlap.
+  const int i0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  int c0 = 0, l0 = 0;
+  if (i0 <= iv.n && lane < k) {
+    c0 = iv.cand[(size_t)i0 * k + lane];
+    l0 = iv.lvl[(size_t)i0 * k + lane];
+  }
+  const uint8_t *tau = cur_tau(pv.tau, et.tau_alt, st);
   if (st) {
     int stop = *(volatile int *)&st->stop_flags;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -255,20 +269,21 @@ __global__ void __launch_bounds__(256) k_weights(InstanceView iv,
     }
     if (stop) return;
   }
-  const int lane = threadIdx.x & 31;
-  const int warps = gridDim.x * (blockDim.x >> 5);
-  const int k = iv.k;
-  const size_t stride = (size_t)iv.n + 1;
-  const uint8_t *tau = cur_tau(pv.tau, et.tau_alt, st);
-  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i <= iv.n;
-       i += warps) {
+  for (int i = i0; i <= iv.n; i += warps) {
     int c = 0;
     int e = INT_MIN;
     if (lane < k) {
-      c = iv.cand[(size_t)i * k + lane];
+      int lv;
+      if (i == i0) {
+        c = c0;
+        lv = l0;
+      } else {
+        c = iv.cand[(size_t)i * k + lane];
+        lv = iv.lvl[(size_t)i * k + lane];
+      }
       if (c > 0) {
         uint8_t q = tau[(size_t)i * stride + c];
-        e = __ldg(et.A + q) - (int)iv.lvl[(size_t)i * k + lane];
+        e = __ldg(et.A + q) - lv;
       }
     }
     int emax = __reduce_max_sync(kFull, e);
